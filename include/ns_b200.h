@@ -1,0 +1,159 @@
+/*
+ * ns_b200.h -- C ABI of the B200-native explicit right-hand side and SSP-RK3
+ * time step of a 3D compressible Navier-Stokes finite-difference solver
+ * (drop-in for the hot path of hamsteri15/3DNSsolver).
+ *
+ * Conventions
+ *   - Every call returns ns_status; no C++ exception crosses this boundary and
+ *     nothing calls exit().  ns_last_error_string() describes the last failure
+ *     on the calling thread.
+ *   - Host arrays at the boundary use the reference container layout
+ *     (src/containers/array_4d.hpp:64-71): AoS [i][j][k][q], q fastest,
+ *     dims (nx+6)(ny+6)(nz+6) x 5 doubles, 3 ghost cells per side
+ *     (src/params.hpp:16-18).  Primitive order is [rho, p, u, v, w]
+ *     (src/domain.hpp:49), conservative order [rho, rhoE, rhou, rhov, rhow]
+ *     (src/domain.hpp:52).  Host pointers are borrowed for the call only.
+ *   - One context per host thread; a context is not thread-safe.  All device
+ *     work of a context is ordered on one CUDA stream (its own, or one adopted
+ *     with ns_set_stream).
+ *   - Device state is owned by the context (SoA FP64 with on-device halos).
+ */
+#ifndef NS_B200_H
+#define NS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NS_ABI_VERSION 1
+#define NS_NGC 3 /* ghost cells per side, src/params.hpp:16-18 */
+#define NS_NQ 5  /* variables per cell, src/domain.cpp:160 */
+
+typedef enum ns_status {
+    NS_OK = 0,
+    NS_ERR_INVALID_ARG = 1,
+    NS_ERR_OOM = 2,
+    NS_ERR_CUDA = 3,
+    NS_ERR_NONFINITE = 4,
+    NS_ERR_TIMEOUT = 5,
+    NS_ERR_UNSUPPORTED = 6,
+    NS_ERR_NO_DEVICE = 7
+} ns_status;
+
+/* ConvectionScheme factory choices, src/driver.cpp:74-94 */
+enum { NS_CONV_NONE = 0, NS_CONV_WENO5 = 1, NS_CONV_WENO5_CHAR = 2 };
+/* WENO weight type, src/convection_schemes/weno-5.cpp:294,313 */
+enum { NS_WEIGHTS_SHU = 0, NS_WEIGHTS_BORGES = 1 };
+/* DiffusionScheme factory choices, src/driver.cpp:96-105 */
+enum { NS_DIFF_NONE = 0, NS_DIFF_CENTERED = 1 };
+/* Per-axis boundary: periodic (MPI_Cart periodic flag, src/decomposition.cpp:116-161)
+ * or zeroth-order Neumann copy (src/boundary_conditions/boundary_neumann.cpp:22-132). */
+enum { NS_BC_PERIODIC = 0, NS_BC_NEUMANN = 1 };
+/* Arithmetic of the stencil / flux / WENO work.  FP32 keeps the RK3
+ * accumulation and all global reductions in FP64. */
+enum { NS_PREC_FP64 = 0, NS_PREC_FP32 = 1 };
+/* NS_SEM_REFERENCE reproduces the reference formulas exactly (including its
+ * non-textbook terms); NS_SEM_PHYSICAL corrects them (no reference counterpart). */
+enum { NS_SEM_REFERENCE = 0, NS_SEM_PHYSICAL = 1 };
+/* Right-hand-side terms for ns_rhs */
+enum { NS_TERM_CONVECTION = 1, NS_TERM_DIFFUSION = 2, NS_TERM_ALL = 3 };
+
+/* Mirrors the hot-path fields of Params (src/params.hpp:20-43). */
+typedef struct ns_params {
+    int dim;             /* Geometry/Dim; dim != 3 skips the z convection sweep (weno-5.cpp:28) */
+    int nx, ny, nz;      /* interior cells per axis */
+    double Lx, Ly, Lz;   /* domain lengths; dx = Lx/nx (src/grid.cpp:12-19) */
+    double mu, Pr, gamma;/* FluidProperties: constant viscosity, Prandtl, ratio of specific heats */
+    double cfl;          /* Time/CFLmax */
+    int convection;      /* NS_CONV_* */
+    int weights;         /* NS_WEIGHTS_* */
+    int diffusion;       /* NS_DIFF_* */
+    int diffusion_order; /* 2, 4 or 6 (src/difference_operators/cd_constants.hpp) */
+    int bc[3];           /* x (West/East), y (North/South), z (Back/Front): NS_BC_* */
+    int precision;       /* NS_PREC_* */
+    int semantics;       /* NS_SEM_* */
+    int sensor;          /* 1: learned sensor gates the characteristic projection (FP32 only) */
+    double sensor_threshold; /* sensor fires when sigmoid(logit) > threshold (default 0.5) */
+    int reserved[8];
+} ns_params;
+
+/* Global diagnostics of the device state (no reference counterpart: the
+ * reference prints dt only, src/driver.cpp:61-64). */
+typedef struct ns_diagnostics {
+    long long steps;     /* steps taken by ns_advance / ns_time_step on this context */
+    double dt;           /* dt of the last step (set_dt, src/time_scheme.cpp:127-136) */
+    double next_dt;      /* dt the next step will use (CFL min over the current state) */
+    double time;         /* sum of dt over the steps taken */
+    double mass;         /* sum rho dV */
+    double momentum[3];  /* sum rho u_d dV */
+    double energy;       /* sum rhoE dV */
+    double kinetic;      /* sum 0.5 rho |u|^2 dV */
+    double enstrophy;    /* sum 0.5 rho |curl u|^2 dV (second-order central curl) */
+    int nonfinite;       /* 1 if any interior conserved value is NaN/Inf */
+    double sensor_fraction; /* fraction of faces the sensor flagged in the last stage */
+} ns_diagnostics;
+
+typedef struct ns_ctx ns_ctx;
+
+const char* ns_status_string(ns_status s);
+/* Message of the last failure on this thread ("" if none). */
+const char* ns_last_error_string(void);
+int ns_abi_version(void);
+
+/* Fills *p with the defaults of the tutorial case (src/io/reader.cpp:3-172 fields). */
+ns_status ns_params_default(ns_params* p);
+
+/* Creates a context and allocates its device state on the current CUDA device.
+ * Replaces Driver::run's construction of Grid/Domain/operators
+ * (src/driver.cpp:9-25) for the hot path. */
+ns_status ns_create(const ns_params* p, ns_ctx** out);
+void ns_destroy(ns_ctx* ctx);
+/* Adopts a caller's cudaStream_t (NULL selects the context's own stream). */
+ns_status ns_set_stream(ns_ctx* ctx, void* cuda_stream);
+/* Number of elements of one host halo'd array: (nx+6)(ny+6)(nz+6)*5. */
+size_t ns_host_array_elems(const ns_params* p);
+
+/* ---- state transfer (host AoS with halos) -------------------------------- */
+/* Sets the primitive state W (Domain::get_NS_primitive_array, src/domain.hpp:36). */
+ns_status ns_upload_primitive(ns_ctx* ctx, const double* W);
+ns_status ns_download_primitive(ns_ctx* ctx, double* W);
+ns_status ns_download_conservative(ns_ctx* ctx, double* U);
+
+/* ---- operator plug-ins (drop-in for the reference virtual interfaces) ----- */
+/* ConvectionScheme::solve(grid, W, U, R) (src/convection_schemes/convection_scheme.hpp:26,
+ * Weno5::solve src/convection_schemes/weno-5.cpp:3-37): R += convective residual.
+ * W and U are read including their halos as given; only R's interior is written. */
+ns_status ns_convection_solve(ns_ctx* ctx, const double* W, const double* U, double* R);
+/* DiffusionScheme::solve(grid, comm, W, R) (src/diffusion_schemes/diffusion_scheme.hpp:14-17,
+ * CenteredDiffusion::solve src/diffusion_schemes/centered_diffusion.cpp:3-68): R += viscous residual.
+ * W is read including its halos as given. */
+ns_status ns_diffusion_solve(ns_ctx* ctx, const double* W, double* R);
+/* First RK stage's right-hand side from a primitive field: prim->cons on all cells,
+ * boundary fill + halo exchange, cons->prim, R = 0, then the selected terms
+ * (src/time_scheme.cpp:124-140).  W is read (halos included), R's interior written. */
+ns_status ns_rhs(ns_ctx* ctx, const double* W, double* R, int terms);
+/* TimeScheme::set_dt (src/time_scheme.cpp:98-136): CFL * min over interior cells. */
+ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out);
+/* TimeScheme::step (src/time_scheme.hpp:25-29, src/time_scheme.cpp:3-70): one SSP-RK3
+ * step of host W (in/out) and U (out, may be NULL); dt_out receives the step's dt.
+ * Host <-> device copies are part of the call. */
+ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out);
+
+/* ---- device-resident time loop -------------------------------------------- */
+/* Runs nsteps steps of TimeScheme::step on the device-resident state (the Driver
+ * loop, src/driver.cpp:43-68, without host copies).  Asynchronous on the
+ * context's stream; no host synchronisation inside. */
+ns_status ns_advance(ns_ctx* ctx, int nsteps);
+/* Blocks until the context's stream is idle; NS_ERR_NONFINITE if
+ * check_finite was requested and the state holds NaN/Inf. */
+ns_status ns_synchronize(ns_ctx* ctx);
+ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
+/* Device kernels launched by this context since creation (for launch accounting). */
+long long ns_kernel_launches(ns_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NS_B200_H */
