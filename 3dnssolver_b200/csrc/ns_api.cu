@@ -1,0 +1,624 @@
+// ns_api.cu -- the C ABI of include/ns_b200.h: context, validation, host
+// transfers and the orchestration of the RK3 stage kernels on one stream.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "ns_common.cuh"
+#include "ns_kernels.h"
+#include "ns_sensor.h"
+
+using namespace nsb;
+
+namespace {
+
+thread_local std::string g_err;
+
+ns_status fail(ns_status s, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
+ns_status fail(ns_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+#define NS_CUDA(call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? NS_ERR_OOM : NS_ERR_CUDA, "%s: %s", \
+                        #call, cudaGetErrorString(e_));                                     \
+    } while (0)
+
+#define NS_TRY(expr)                 \
+    do {                             \
+        ns_status s_ = (expr);       \
+        if (s_ != NS_OK) return s_;  \
+    } while (0)
+
+}  // namespace
+
+struct ns_ctx {
+    ns_params p;
+    Box box;
+    FaceBox fb[3];
+    Consts c;
+    int device = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    double* W = nullptr;   // primitive, halo'd SoA
+    double* U = nullptr;   // conservative, halo'd SoA
+    double* U0 = nullptr;  // RK stage base (interior used)
+    double* R = nullptr;   // residual for the operator entry points (lazy)
+    void* F[3] = {nullptr, nullptr, nullptr};
+    double* stage = nullptr;              // host-layout staging (lazy)
+    unsigned long long* slot = nullptr;   // [0]: CFL min of the current step, [1]: scratch
+    double* diag = nullptr;               // [8] diagnostics sums
+    double* clock = nullptr;              // [2] last dt, accumulated time
+    bool w_valid = false, u_valid = false;
+    long long steps = 0;
+    long long launches = 0;
+    nsb::SensorState* sensor = nullptr;
+    double last_sensor_fraction = 0.0;
+};
+
+static size_t host_elems(const ns_params* p) {
+    return (size_t)(p->nx + 2 * NS_NGC) * (p->ny + 2 * NS_NGC) * (p->nz + 2 * NS_NGC) * NS_NQ;
+}
+
+static ns_status validate(const ns_params* p) {
+    if (!p) return fail(NS_ERR_INVALID_ARG, "params is NULL");
+    if (p->dim != 2 && p->dim != 3) return fail(NS_ERR_INVALID_ARG, "dim must be 2 or 3 (got %d)", p->dim);
+    if (p->nx < 3 || p->ny < 3 || p->nz < 1 || (p->dim == 3 && p->nz < 3))
+        return fail(NS_ERR_INVALID_ARG,
+                    "grid %dx%dx%d: need nx, ny >= 3 and nz >= 3 when dim == 3 (3 ghost cells per side)",
+                    p->nx, p->ny, p->nz);
+    if ((long long)p->nx + 6 > 65535)
+        return fail(NS_ERR_INVALID_ARG, "nx = %d exceeds the launch grid limit", p->nx);
+    if (!(p->Lx > 0 && p->Ly > 0 && p->Lz > 0)) return fail(NS_ERR_INVALID_ARG, "domain lengths must be > 0");
+    if (!(p->gamma > 1.0)) return fail(NS_ERR_INVALID_ARG, "gamma must be > 1");
+    if (!(p->mu >= 0.0)) return fail(NS_ERR_INVALID_ARG, "mu must be >= 0");
+    if (!(p->Pr > 0.0)) return fail(NS_ERR_INVALID_ARG, "Pr must be > 0");
+    if (!(p->cfl > 0.0)) return fail(NS_ERR_INVALID_ARG, "cfl must be > 0");
+    if (p->convection < NS_CONV_NONE || p->convection > NS_CONV_WENO5_CHAR)
+        return fail(NS_ERR_INVALID_ARG, "unknown convection scheme %d", p->convection);
+    if (p->weights != NS_WEIGHTS_SHU && p->weights != NS_WEIGHTS_BORGES)
+        return fail(NS_ERR_INVALID_ARG, "unknown WENO weight type %d", p->weights);
+    if (p->diffusion != NS_DIFF_NONE && p->diffusion != NS_DIFF_CENTERED)
+        return fail(NS_ERR_INVALID_ARG, "unknown diffusion scheme %d", p->diffusion);
+    if (p->diffusion_order != 2 && p->diffusion_order != 4 && p->diffusion_order != 6)
+        return fail(NS_ERR_INVALID_ARG, "diffusion order must be 2, 4 or 6 (got %d)", p->diffusion_order);
+    for (int a = 0; a < 3; a++)
+        if (p->bc[a] != NS_BC_PERIODIC && p->bc[a] != NS_BC_NEUMANN)
+            return fail(NS_ERR_INVALID_ARG, "unknown boundary type %d on axis %d", p->bc[a], a);
+    if (p->precision != NS_PREC_FP64 && p->precision != NS_PREC_FP32)
+        return fail(NS_ERR_INVALID_ARG, "unknown precision %d", p->precision);
+    if (p->semantics != NS_SEM_REFERENCE && p->semantics != NS_SEM_PHYSICAL)
+        return fail(NS_ERR_INVALID_ARG, "unknown semantics %d", p->semantics);
+    if (p->sensor) {
+        if (p->convection != NS_CONV_WENO5_CHAR)
+            return fail(NS_ERR_INVALID_ARG, "the sensor gates the characteristic scheme: convection must be NS_CONV_WENO5_CHAR");
+        if (p->precision != NS_PREC_FP32)
+            return fail(NS_ERR_INVALID_ARG, "the sensor-gated form runs in NS_PREC_FP32");
+        if (!(p->sensor_threshold > 0.0 && p->sensor_threshold < 1.0))
+            return fail(NS_ERR_INVALID_ARG, "sensor_threshold must lie in (0,1)");
+    }
+    return NS_OK;
+}
+
+static Consts make_consts(const ns_params* p) {
+    // CD coefficients, src/difference_operators/cd_constants.hpp:10-28 (centred at index 3)
+    static const double cd2_df[3] = {-1. / 2, 0., 1. / 2.};
+    static const double cd2_ddf[3] = {1., -2., 1.};
+    static const double cd4_df[5] = {1. / 12., -2. / 3., 0., 2. / 3., -1. / 12.};
+    static const double cd4_ddf[5] = {-1. / 12., 4. / 3., -5. / 2., 4. / 3., -1. / 12.};
+    static const double cd6_df[7] = {-1. / 60., 3. / 20., -3. / 4., 0., 3. / 4., -3. / 20., 1. / 60.};
+    static const double cd6_ddf[7] = {1. / 90., -3. / 20., 3. / 2., -49. / 18., 3. / 2., -3. / 20., 1. / 90.};
+    Consts c;
+    memset(&c, 0, sizeof c);
+    c.gamma = p->gamma;
+    c.gm1 = p->gamma - 1.0;
+    c.inv_gm1 = 1.0 / (p->gamma - 1.0);
+    c.mu = p->mu;
+    c.lamb = (-2. / 3.) * p->mu;
+    c.heat = p->gamma / (p->Pr * (p->gamma - 1.0));
+    c.dx = p->Lx / p->nx;
+    c.dy = p->Ly / p->ny;
+    c.dz = p->Lz / p->nz;
+    c.inv_dx = 1.0 / c.dx;
+    c.inv_dy = 1.0 / c.dy;
+    c.inv_dz = 1.0 / c.dz;
+    c.cfl = p->cfl;
+    for (int a = 0; a < 3; a++) c.periodic[a] = (p->bc[a] == NS_BC_PERIODIC);
+    c.dim = p->dim;
+    c.order = p->diffusion_order;
+    const double *df = cd2_df, *ddf = cd2_ddf;
+    int w = 3;
+    if (p->diffusion_order == 4) { df = cd4_df; ddf = cd4_ddf; w = 5; }
+    if (p->diffusion_order == 6) { df = cd6_df; ddf = cd6_ddf; w = 7; }
+    int h = w / 2;
+    for (int t = 0; t < w; t++) {
+        c.df[3 - h + t] = df[t];
+        c.ddf[3 - h + t] = ddf[t];
+    }
+    return c;
+}
+
+static size_t soa_bytes(const Box& b) { return (size_t)b.fstride * NS_NQ * sizeof(double); }
+
+static ns_status check_launch(ns_ctx* ctx, int n) {
+    ctx->launches += n;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(NS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return NS_OK;
+}
+
+static ns_status ensure_stage(ns_ctx* ctx) {
+    if (!ctx->stage) NS_CUDA(cudaMalloc(&ctx->stage, host_elems(&ctx->p) * sizeof(double)));
+    return NS_OK;
+}
+
+static ns_status ensure_R(ns_ctx* ctx) {
+    if (!ctx->R) {
+        NS_CUDA(cudaMalloc(&ctx->R, soa_bytes(ctx->box)));
+        NS_CUDA(cudaMemsetAsync(ctx->R, 0, soa_bytes(ctx->box), ctx->stream));
+    }
+    return NS_OK;
+}
+
+static ns_status upload(ns_ctx* ctx, const double* host, double* dev) {
+    if (!host) return fail(NS_ERR_INVALID_ARG, "host array is NULL");
+    NS_TRY(ensure_stage(ctx));
+    NS_CUDA(cudaMemcpyAsync(ctx->stage, host, host_elems(&ctx->p) * sizeof(double),
+                            cudaMemcpyHostToDevice, ctx->stream));
+    launch_aos_to_soa(ctx->stage, dev, ctx->box, ctx->stream);
+    return check_launch(ctx, 1);
+}
+
+static ns_status download(ns_ctx* ctx, const double* dev, double* host) {
+    if (!host) return fail(NS_ERR_INVALID_ARG, "host array is NULL");
+    NS_TRY(ensure_stage(ctx));
+    launch_soa_to_aos(dev, ctx->stage, ctx->box, ctx->stream);
+    NS_TRY(check_launch(ctx, 1));
+    NS_CUDA(cudaMemcpyAsync(host, ctx->stage, host_elems(&ctx->p) * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return NS_OK;
+}
+
+static bool phys(const ns_ctx* ctx) { return ctx->p.semantics == NS_SEM_PHYSICAL; }
+static bool fp32(const ns_ctx* ctx) { return ctx->p.precision == NS_PREC_FP32; }
+
+// optional event trail for ns_profile_step: an event after every kernel, tagged
+// with the kernel class it closes
+struct Prof {
+    cudaEvent_t ev[64];
+    int cls[64];
+    int n = 0;
+};
+static Prof* g_prof = nullptr;  // set only inside ns_profile_step (single-threaded per context)
+
+static void prof_mark(ns_ctx* ctx, int cls) {
+    if (!g_prof || g_prof->n >= 64) return;
+    cudaEventRecord(g_prof->ev[g_prof->n], ctx->stream);
+    g_prof->cls[g_prof->n++] = cls;
+}
+
+// face fluxes of the current (W, U) along every convected axis
+static ns_status faces(ns_ctx* ctx) {
+    const ns_params& p = ctx->p;
+    if (p.convection == NS_CONV_NONE) return NS_OK;
+    int nd = p.dim == 3 ? 3 : 2;
+    for (int d = 0; d < nd; d++) {
+        if (p.sensor) {
+            NS_TRY(sensor_face_flux(ctx->sensor, d, ctx->W, ctx->U, ctx->box, ctx->c, ctx->F[d],
+                                    ctx->fb[d], ctx->stream, &ctx->launches));
+        } else {
+            launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
+                             phys(ctx), fp32(ctx), ctx->W, ctx->U, ctx->box, ctx->c, ctx->F[d],
+                             ctx->fb[d], ctx->stream);
+            NS_TRY(check_launch(ctx, 1));
+        }
+        prof_mark(ctx, NS_PROF_FACE_X + d);
+    }
+    return NS_OK;
+}
+
+static UpdateArgs update_args(ns_ctx* ctx, int mode, bool conv, bool visc) {
+    UpdateArgs a;
+    memset(&a, 0, sizeof a);
+    a.W = ctx->W;
+    a.U = ctx->U;
+    a.U0 = ctx->U0;
+    for (int d = 0; d < 3; d++) { a.F[d] = ctx->F[d]; a.fb[d] = ctx->fb[d]; }
+    a.b = ctx->box;
+    a.c = ctx->c;
+    a.flags = 0;
+    if (conv && ctx->p.convection != NS_CONV_NONE) {
+        a.flags |= UPD_CONV;
+        if (ctx->p.dim == 3) a.flags |= UPD_CONVZ;
+    }
+    a.mode = mode;
+    a.viscous = visc && ctx->p.diffusion == NS_DIFF_CENTERED;
+    a.phys = phys(ctx);
+    a.fp32 = fp32(ctx);
+    a.slot = ctx->slot;
+    a.Rout = ctx->R;
+    return a;
+}
+
+// one TimeScheme::step on the device state
+static ns_status do_step(ns_ctx* ctx) {
+    cudaStream_t s = ctx->stream;
+    NS_CUDA(cudaMemsetAsync(ctx->slot, 0xFF, sizeof(unsigned long long), s));
+    launch_step_begin(!ctx->w_valid, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, ctx->slot, s);
+    NS_TRY(check_launch(ctx, 1));
+    prof_mark(ctx, NS_PROF_STEP_BEGIN);
+    // SSP-RK3 coefficients (time_scheme.cpp:36-38, 48-50, 60-62)
+    const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
+    const double m2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
+    const double mc[3] = {-1.0, -(1. / 4.), -(2. / 3.)};
+    for (int st = 0; st < 3; st++) {
+        launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
+        NS_TRY(check_launch(ctx, 1));
+        prof_mark(ctx, NS_PROF_FILL);
+        NS_TRY(faces(ctx));
+        UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
+        a.m1 = m1[st];
+        a.m2 = m2[st];
+        a.mc = mc[st];
+        a.clock = (st == 0) ? ctx->clock : nullptr;
+        launch_update(a, s);
+        NS_TRY(check_launch(ctx, 1));
+        prof_mark(ctx, NS_PROF_UPDATE);
+    }
+    ctx->u_valid = true;
+    ctx->w_valid = false;
+    ctx->steps++;
+    return NS_OK;
+}
+
+static ns_status finalize_w(ns_ctx* ctx) {
+    if (!ctx->w_valid) {
+        launch_prim_all(ctx->W, ctx->U, ctx->box, ctx->c, ctx->stream);
+        NS_TRY(check_launch(ctx, 1));
+        ctx->w_valid = true;
+    }
+    return NS_OK;
+}
+
+static double slot_dt(unsigned long long bits, double cfl) {
+    double v;
+    memcpy(&v, &bits, sizeof v);
+    return fmin(1e10, v) * cfl;
+}
+
+// ===========================================================================
+extern "C" {
+
+const char* ns_status_string(ns_status s) {
+    switch (s) {
+        case NS_OK: return "ok";
+        case NS_ERR_INVALID_ARG: return "invalid argument";
+        case NS_ERR_OOM: return "out of device memory";
+        case NS_ERR_CUDA: return "CUDA error";
+        case NS_ERR_NONFINITE: return "non-finite state";
+        case NS_ERR_TIMEOUT: return "device wait timed out";
+        case NS_ERR_UNSUPPORTED: return "unsupported";
+        case NS_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char* ns_last_error_string(void) { return g_err.c_str(); }
+
+int ns_abi_version(void) { return NS_ABI_VERSION; }
+
+size_t ns_host_array_elems(const ns_params* p) { return p ? host_elems(p) : 0; }
+
+ns_status ns_params_default(ns_params* p) {
+    if (!p) return fail(NS_ERR_INVALID_ARG, "params is NULL");
+    memset(p, 0, sizeof *p);
+    // tutorials/shearLayer/input.xml values, 3D
+    p->dim = 3;
+    p->nx = p->ny = p->nz = 64;
+    p->Lx = p->Ly = p->Lz = 1.0;
+    p->mu = 1e-4;
+    p->Pr = 0.71;
+    p->gamma = 1.4;
+    p->cfl = 0.4;
+    p->convection = NS_CONV_WENO5;
+    p->weights = NS_WEIGHTS_SHU;
+    p->diffusion = NS_DIFF_CENTERED;
+    p->diffusion_order = 2;
+    p->bc[0] = p->bc[1] = p->bc[2] = NS_BC_PERIODIC;
+    p->precision = NS_PREC_FP64;
+    p->semantics = NS_SEM_REFERENCE;
+    p->sensor = 0;
+    p->sensor_threshold = 0.5;
+    return NS_OK;
+}
+
+void ns_destroy(ns_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->W);
+    cudaFree(ctx->U);
+    cudaFree(ctx->U0);
+    cudaFree(ctx->R);
+    for (int d = 0; d < 3; d++) cudaFree(ctx->F[d]);
+    cudaFree(ctx->stage);
+    cudaFree(ctx->slot);
+    cudaFree(ctx->diag);
+    cudaFree(ctx->clock);
+    if (ctx->sensor) sensor_destroy(ctx->sensor);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+}
+
+ns_status ns_create(const ns_params* p, ns_ctx** out) {
+    if (!out) return fail(NS_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    NS_TRY(validate(p));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(NS_ERR_NO_DEVICE, "no CUDA device is visible");
+    }
+    ns_ctx* ctx = new (std::nothrow) ns_ctx();
+    if (!ctx) return fail(NS_ERR_OOM, "host allocation failed");
+    ctx->p = *p;
+    ctx->box = make_box(p->nx, p->ny, p->nz);
+    for (int d = 0; d < 3; d++) ctx->fb[d] = make_facebox(p->nx, p->ny, p->nz, d);
+    ctx->c = make_consts(p);
+    cudaGetDevice(&ctx->device);
+    ns_status st = NS_OK;
+    auto A = [&](void** ptr, size_t bytes) {
+        if (st != NS_OK) return;
+        cudaError_t e = cudaMalloc(ptr, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(e == cudaErrorMemoryAllocation ? NS_ERR_OOM : NS_ERR_CUDA,
+                      "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+        }
+    };
+    if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
+        ns_destroy(ctx);
+        return fail(NS_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    ctx->stream = ctx->own;
+    A((void**)&ctx->W, soa_bytes(ctx->box));
+    A((void**)&ctx->U, soa_bytes(ctx->box));
+    A((void**)&ctx->U0, soa_bytes(ctx->box));
+    size_t fe = fp32(ctx) ? sizeof(float) : sizeof(double);
+    if (p->convection != NS_CONV_NONE)
+        for (int d = 0; d < (p->dim == 3 ? 3 : 2); d++)
+            A(&ctx->F[d], (size_t)ctx->fb[d].fstride * NS_NQ * fe);
+    A((void**)&ctx->slot, 2 * sizeof(unsigned long long));
+    A((void**)&ctx->diag, 8 * sizeof(double));
+    A((void**)&ctx->clock, 2 * sizeof(double));
+    if (st == NS_OK) {
+        // zero the state so halos/corners hold defined values before the first upload
+        cudaMemsetAsync(ctx->W, 0, soa_bytes(ctx->box), ctx->stream);
+        cudaMemsetAsync(ctx->U, 0, soa_bytes(ctx->box), ctx->stream);
+        cudaMemsetAsync(ctx->U0, 0, soa_bytes(ctx->box), ctx->stream);
+        cudaMemsetAsync(ctx->clock, 0, 2 * sizeof(double), ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            st = fail(NS_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    if (st == NS_OK && p->sensor) st = sensor_create(&ctx->sensor, ctx->box, ctx->fb, ctx->stream);
+    if (st != NS_OK) {
+        ns_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return NS_OK;
+}
+
+ns_status ns_set_stream(ns_ctx* ctx, void* stream) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->own;
+    if (s != ctx->stream) {
+        // order the new stream after everything queued on the old one
+        cudaEvent_t ev;
+        NS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        NS_CUDA(cudaEventRecord(ev, ctx->stream));
+        NS_CUDA(cudaStreamWaitEvent(s, ev, 0));
+        cudaEventDestroy(ev);
+        ctx->stream = s;
+    }
+    return NS_OK;
+}
+
+ns_status ns_upload_primitive(ns_ctx* ctx, const double* W) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    NS_TRY(upload(ctx, W, ctx->W));
+    ctx->w_valid = true;
+    ctx->u_valid = false;
+    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return NS_OK;
+}
+
+ns_status ns_download_primitive(ns_ctx* ctx, double* W) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!ctx->w_valid && !ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no state has been uploaded");
+    NS_TRY(finalize_w(ctx));
+    return download(ctx, ctx->W, W);
+}
+
+ns_status ns_download_conservative(ns_ctx* ctx, double* U) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no conservative state yet (take a step first)");
+    return download(ctx, ctx->U, U);
+}
+
+ns_status ns_convection_solve(ns_ctx* ctx, const double* W, const double* U, double* R) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!W || !U || !R) return fail(NS_ERR_INVALID_ARG, "W, U and R must be non-NULL");
+    NS_TRY(ensure_R(ctx));
+    NS_TRY(upload(ctx, W, ctx->W));
+    NS_TRY(upload(ctx, U, ctx->U));
+    NS_TRY(upload(ctx, R, ctx->R));
+    ctx->w_valid = ctx->u_valid = false;  // the device state now holds the operator's inputs
+    NS_TRY(faces(ctx));
+    UpdateArgs a = update_args(ctx, MODE_RHS, true, false);
+    launch_update(a, ctx->stream);
+    NS_TRY(check_launch(ctx, 1));
+    return download(ctx, ctx->R, R);
+}
+
+ns_status ns_diffusion_solve(ns_ctx* ctx, const double* W, double* R) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!W || !R) return fail(NS_ERR_INVALID_ARG, "W and R must be non-NULL");
+    NS_TRY(ensure_R(ctx));
+    NS_TRY(upload(ctx, W, ctx->W));
+    NS_TRY(upload(ctx, R, ctx->R));
+    ctx->w_valid = ctx->u_valid = false;
+    UpdateArgs a = update_args(ctx, MODE_RHS, false, true);
+    launch_update(a, ctx->stream);
+    NS_TRY(check_launch(ctx, 1));
+    return download(ctx, ctx->R, R);
+}
+
+ns_status ns_rhs(ns_ctx* ctx, const double* W, double* R, int terms) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!W || !R) return fail(NS_ERR_INVALID_ARG, "W and R must be non-NULL");
+    if (terms < 0 || terms > NS_TERM_ALL) return fail(NS_ERR_INVALID_ARG, "terms must be a mask of NS_TERM_*");
+    NS_TRY(ensure_R(ctx));
+    NS_TRY(upload(ctx, W, ctx->W));
+    NS_TRY(upload(ctx, R, ctx->R));
+    cudaStream_t s = ctx->stream;
+    NS_CUDA(cudaMemsetAsync(ctx->slot, 0xFF, sizeof(unsigned long long), s));
+    launch_step_begin(false, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, ctx->slot, s);
+    launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
+    NS_TRY(check_launch(ctx, 2));
+    if (terms & NS_TERM_CONVECTION) NS_TRY(faces(ctx));
+    UpdateArgs a = update_args(ctx, MODE_RHS, terms & NS_TERM_CONVECTION, terms & NS_TERM_DIFFUSION);
+    a.flags |= UPD_OVERWRITE;
+    launch_update(a, s);
+    NS_TRY(check_launch(ctx, 1));
+    ctx->w_valid = ctx->u_valid = false;
+    return download(ctx, ctx->R, R);
+}
+
+ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!dt_out) return fail(NS_ERR_INVALID_ARG, "dt_out is NULL");
+    NS_TRY(upload(ctx, W, ctx->W));
+    ctx->w_valid = true;
+    ctx->u_valid = false;
+    NS_CUDA(cudaMemsetAsync(ctx->slot + 1, 0xFF, sizeof(unsigned long long), ctx->stream));
+    launch_min_dt(phys(ctx), ctx->W, ctx->box, ctx->c, ctx->slot + 1, ctx->stream);
+    NS_TRY(check_launch(ctx, 1));
+    unsigned long long bits;
+    NS_CUDA(cudaMemcpyAsync(&bits, ctx->slot + 1, sizeof bits, cudaMemcpyDeviceToHost, ctx->stream));
+    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    *dt_out = slot_dt(bits, ctx->p.cfl);
+    return NS_OK;
+}
+
+ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!W) return fail(NS_ERR_INVALID_ARG, "W is NULL");
+    NS_TRY(upload(ctx, W, ctx->W));
+    ctx->w_valid = true;
+    ctx->u_valid = false;
+    NS_TRY(do_step(ctx));
+    NS_TRY(finalize_w(ctx));
+    unsigned long long bits;
+    NS_CUDA(cudaMemcpyAsync(&bits, ctx->slot, sizeof bits, cudaMemcpyDeviceToHost, ctx->stream));
+    NS_TRY(download(ctx, ctx->W, W));
+    if (U) NS_TRY(download(ctx, ctx->U, U));
+    if (dt_out) *dt_out = slot_dt(bits, ctx->p.cfl);
+    return NS_OK;
+}
+
+ns_status ns_advance(ns_ctx* ctx, int nsteps) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (nsteps < 0) return fail(NS_ERR_INVALID_ARG, "nsteps must be >= 0");
+    if (!ctx->w_valid && !ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no state has been uploaded");
+    for (int n = 0; n < nsteps; n++) NS_TRY(do_step(ctx));
+    return NS_OK;
+}
+
+ns_status ns_synchronize(ns_ctx* ctx) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return NS_OK;
+}
+
+ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out) {
+    if (!ctx || !out) return fail(NS_ERR_INVALID_ARG, "ctx and out must be non-NULL");
+    memset(out, 0, sizeof *out);
+    out->steps = ctx->steps;
+    if (!ctx->w_valid && !ctx->u_valid) return NS_OK;
+    cudaStream_t s = ctx->stream;
+    NS_TRY(finalize_w(ctx));
+    if (!ctx->u_valid) {
+        // conservative view of an uploaded primitive state (no step taken yet)
+        launch_cons_all(ctx->W, ctx->U, ctx->box, ctx->c, s);
+        NS_TRY(check_launch(ctx, 1));
+        ctx->u_valid = true;
+    }
+    NS_CUDA(cudaMemsetAsync(ctx->diag, 0, 8 * sizeof(double), s));
+    launch_diagnostics(ctx->U, ctx->box, ctx->c, ctx->diag, s);
+    NS_CUDA(cudaMemsetAsync(ctx->slot + 1, 0xFF, sizeof(unsigned long long), s));
+    launch_min_dt(phys(ctx), ctx->W, ctx->box, ctx->c, ctx->slot + 1, s);
+    NS_TRY(check_launch(ctx, 2));
+    double h[8], clk[2];
+    unsigned long long bits[2];
+    NS_CUDA(cudaMemcpyAsync(h, ctx->diag, sizeof h, cudaMemcpyDeviceToHost, s));
+    NS_CUDA(cudaMemcpyAsync(clk, ctx->clock, sizeof clk, cudaMemcpyDeviceToHost, s));
+    NS_CUDA(cudaMemcpyAsync(bits, ctx->slot, sizeof bits, cudaMemcpyDeviceToHost, s));
+    NS_CUDA(cudaStreamSynchronize(s));
+    out->dt = clk[0];
+    out->time = clk[1];
+    out->next_dt = slot_dt(bits[1], ctx->p.cfl);
+    out->mass = h[0];
+    out->momentum[0] = h[1];
+    out->momentum[1] = h[2];
+    out->momentum[2] = h[3];
+    out->energy = h[4];
+    out->kinetic = h[5];
+    out->enstrophy = h[6];
+    out->nonfinite = h[7] > 0 ? 1 : 0;
+    out->sensor_fraction = ctx->sensor ? sensor_last_fraction(ctx->sensor) : 0.0;
+    return NS_OK;
+}
+
+ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
+    if (!ctx || !ms || n < NS_PROF_N) return fail(NS_ERR_INVALID_ARG, "ctx/ms invalid or n < NS_PROF_N");
+    if (!ctx->w_valid && !ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no state has been uploaded");
+    Prof pr;
+    for (int e = 0; e < 64; e++) NS_CUDA(cudaEventCreate(&pr.ev[e]));
+    cudaEvent_t start;
+    NS_CUDA(cudaEventCreate(&start));
+    NS_CUDA(cudaEventRecord(start, ctx->stream));
+    g_prof = &pr;
+    ns_status st = do_step(ctx);
+    g_prof = nullptr;
+    if (st == NS_OK) st = (cudaStreamSynchronize(ctx->stream) == cudaSuccess)
+                              ? NS_OK : fail(NS_ERR_CUDA, "profiled step failed");
+    for (int c = 0; c < n; c++) ms[c] = 0.f;
+    cudaEvent_t prev = start;
+    for (int e = 0; e < pr.n && st == NS_OK; e++) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, prev, pr.ev[e]);
+        ms[pr.cls[e]] += t;
+        prev = pr.ev[e];
+    }
+    for (int e = 0; e < 64; e++) cudaEventDestroy(pr.ev[e]);
+    cudaEventDestroy(start);
+    return st;
+}
+
+long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,186 @@
+// ns_common.cuh -- device layout and shared device helpers.
+//
+// Device state layout (HBM): structure of arrays, one plane per variable,
+// each plane the halo'd box (nx+6) x (ny+6) x NZp doubles with k fastest.
+// NZp = nz+6 rounded up to 8 and every plane starts 5 doubles past a 64-byte
+// boundary, so the first interior cell of every k-row (k = 3) is 64-byte
+// aligned and a warp reading 32 consecutive k touches whole 32-byte sectors.
+// Halos are real storage: the boundary fill writes them (the single-GPU form
+// of Domain::apply_boundary_conditions + Communicator::communicate), and the
+// per-operator entry points accept a caller's halos verbatim.
+#pragma once
+
+#include <cstdint>
+
+#include "../../include/ns_b200.h"
+
+#define NS_HOST_DEVICE __host__ __device__ __forceinline__
+
+namespace nsb {
+
+constexpr int NG = 3;
+constexpr int NQV = 5;
+constexpr int PLANE_PAD = 5;  // elements before interior k=3 reaches 64-byte alignment
+
+struct Box {
+    int nx, ny, nz;     // interior cells
+    int NX, NY, NZp;    // halo'd extents (NZp padded)
+    long long fstride;  // elements per variable plane (incl. alignment pad)
+
+    NS_HOST_DEVICE long long at(int ih, int jh, int kh) const {
+        return ((long long)ih * NY + jh) * NZp + kh;
+    }
+};
+
+inline Box make_box(int nx, int ny, int nz) {
+    Box b;
+    b.nx = nx; b.ny = ny; b.nz = nz;
+    b.NX = nx + 2 * NG; b.NY = ny + 2 * NG;
+    b.NZp = ((nz + 2 * NG + 7) / 8) * 8;
+    long long plane = (long long)b.NX * b.NY * b.NZp;
+    b.fstride = ((plane + PLANE_PAD + 7) / 8) * 8;
+    return b;
+}
+
+// Face arrays: one plane per variable of (n_d+1) faces along the sweep axis,
+// interior extent in the other two, k fastest.  Face f along an axis lies
+// between interior cells f-1 and f.
+struct FaceBox {
+    int n0, n1, n2;     // extents (i or face, j or face, k or face)
+    long long fstride;
+    NS_HOST_DEVICE long long at(int a, int b, int c) const {
+        return ((long long)a * n1 + b) * n2 + c;
+    }
+};
+
+inline FaceBox make_facebox(int nx, int ny, int nz, int dir) {
+    FaceBox f;
+    f.n0 = nx + (dir == 0);
+    f.n1 = ny + (dir == 1);
+    f.n2 = nz + (dir == 2);
+    f.fstride = (((long long)f.n0 * f.n1 * f.n2 + 31) / 32) * 32;
+    return f;
+}
+
+// Kernel-side constants derived from ns_params.
+struct Consts {
+    double gamma, gm1, inv_gm1;
+    double mu, lamb, heat;      // lamb = -2/3 mu, heat = gamma/(Pr(gamma-1))
+    double dx, dy, dz, inv_dx, inv_dy, inv_dz;
+    double cfl;
+    int periodic[3];
+    int dim;
+    int order;                  // CD order 2/4/6
+    double df[7], ddf[7];       // CD coefficients, centred at index 3
+};
+
+// Periodic wrap or Neumann clamp of an interior-coordinate index.
+NS_HOST_DEVICE int fold(int i, int n, int periodic) {
+    if (i >= 0 && i < n) return i;
+    if (periodic) {
+        int r = i % n;
+        return r < 0 ? r + n : r;
+    }
+    return i < 0 ? 0 : n - 1;
+}
+
+// ---------------------------------------------------------------------------
+// WENO-5 (Jiang-Shu smoothness indicators, src/convection_schemes/weno-5.cpp:222-322)
+//
+// The three nonlinear weights are formed with a single division: with
+// s_k = eps + beta_k (Shu) the weights d_k/s_k^2 normalised by their sum equal
+// d_k * prod_{j!=k} s_j^2 / sum_m d_m prod_{j!=m} s_j^2 (Borges: d_k (B_k+tau) prod_{j!=k} B_j).
+// The algebra is exact; results differ from the reference's three-division
+// form by rounding only.  Single precision keeps per-weight reciprocals
+// (products of squares would leave the float range) and raises eps above the
+// float rounding floor of beta: eps32 = max(eps, (8 u32 s)^2), s the largest
+// |f| of the stencil.
+
+template <typename T>
+struct WenoC;
+template <>
+struct WenoC<double> {
+    static constexpr double eps_shu = 1e-6, eps_borges = 1e-14;
+};
+template <>
+struct WenoC<float> {
+    static constexpr float eps_shu = 1e-6f, eps_borges = 1e-14f;
+};
+
+template <typename T>
+__device__ __forceinline__ void weno_betas(T a, T b, T c, T d, T e, T& b0, T& b1, T& b2) {
+    const T k1312 = T(13) / T(12), k14 = T(0.25);
+    T t1 = a - T(2) * b + c, t2 = a - T(4) * b + T(3) * c;
+    b0 = k1312 * t1 * t1 + k14 * t2 * t2;
+    t1 = b - T(2) * c + d;
+    t2 = b - d;
+    b1 = k1312 * t1 * t1 + k14 * t2 * t2;
+    t1 = c - T(2) * d + e;
+    t2 = T(3) * c - T(4) * d + e;
+    b2 = k1312 * t1 * t1 + k14 * t2 * t2;
+}
+
+// Weighted combination of the three candidate values f0,f1,f2 with linear
+// weights (d0,d1,d2) given the stencil (a..e).
+template <typename T, bool BORGES>
+__device__ __forceinline__ T weno_combine(T a, T b, T c, T d, T e, T f0, T f1, T f2, T d0, T d1, T d2) {
+    T b0, b1, b2;
+    weno_betas(a, b, c, d, e, b0, b1, b2);
+    if constexpr (sizeof(T) == 8) {
+        T n0, n1, n2;
+        if constexpr (BORGES) {
+            T tau = fabs(b0 - b2);
+            T B0 = b0 + WenoC<T>::eps_borges, B1 = b1 + WenoC<T>::eps_borges,
+              B2 = b2 + WenoC<T>::eps_borges;
+            n0 = d0 * (B0 + tau) * (B1 * B2);
+            n1 = d1 * (B1 + tau) * (B0 * B2);
+            n2 = d2 * (B2 + tau) * (B0 * B1);
+        } else {
+            T s0 = WenoC<T>::eps_shu + b0, s1 = WenoC<T>::eps_shu + b1, s2 = WenoC<T>::eps_shu + b2;
+            T A0 = s0 * s0, A1 = s1 * s1, A2 = s2 * s2;
+            n0 = d0 * (A1 * A2);
+            n1 = d1 * (A0 * A2);
+            n2 = d2 * (A0 * A1);
+        }
+        return (n0 * f0 + n1 * f1 + n2 * f2) / (n0 + n1 + n2);
+    } else {
+        T a0, a1, a2;
+        if constexpr (BORGES) {
+            T tau = fabsf(b0 - b2);
+            a0 = d0 * (T(1) + tau * __frcp_rn(b0 + WenoC<T>::eps_borges));
+            a1 = d1 * (T(1) + tau * __frcp_rn(b1 + WenoC<T>::eps_borges));
+            a2 = d2 * (T(1) + tau * __frcp_rn(b2 + WenoC<T>::eps_borges));
+        } else {
+            T s = fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fabsf(d))), fabsf(e));
+            T fl = T(8) * T(5.9604645e-8) * s;
+            T eps = fmaxf(WenoC<T>::eps_shu, fl * fl);
+            T s0 = eps + b0, s1 = eps + b1, s2 = eps + b2;
+            a0 = d0 * __frcp_rn(s0 * s0);
+            a1 = d1 * __frcp_rn(s1 * s1);
+            a2 = d2 * __frcp_rn(s2 * s2);
+        }
+        return (a0 * f0 + a1 * f1 + a2 * f2) * __frcp_rn(a0 + a1 + a2);
+    }
+}
+
+// WENO5_left (weno-5.cpp:305-322): value at i+1/2 from the left-biased stencil a..e = i-2..i+2
+template <typename T, bool BORGES>
+__device__ __forceinline__ T weno_left(T a, T b, T c, T d, T e) {
+    const T s6 = T(1) / T(6);
+    T f0 = (T(2) * a - T(7) * b + T(11) * c) * s6;
+    T f1 = (-b + T(5) * c + T(2) * d) * s6;
+    T f2 = (T(2) * c + T(5) * d - e) * s6;
+    return weno_combine<T, BORGES>(a, b, c, d, e, f0, f1, f2, T(0.1), T(0.6), T(0.3));
+}
+
+// WENO5_right (weno-5.cpp:285-303): value at i+1/2 from the right-biased stencil a..e = i-1..i+3
+template <typename T, bool BORGES>
+__device__ __forceinline__ T weno_right(T a, T b, T c, T d, T e) {
+    const T s6 = T(1) / T(6);
+    T f0 = (-a + T(5) * b + T(2) * c) * s6;
+    T f1 = (T(2) * b + T(5) * c - d) * s6;
+    T f2 = (T(11) * c - T(7) * d + T(2) * e) * s6;
+    return weno_combine<T, BORGES>(a, b, c, d, e, f0, f1, f2, T(0.3), T(0.6), T(0.1));
+}
+
+}  // namespace nsb

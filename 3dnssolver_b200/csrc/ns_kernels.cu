@@ -1,0 +1,883 @@
+// ns_kernels.cu -- device kernels of the explicit RHS and SSP-RK3 stage.
+//
+// Per RK stage (TimeScheme::step, src/time_scheme.cpp:33-66):
+//   k_fill_prim      boundary fill + halo exchange of U on the face halos, then
+//                    W = prim(U) on every cell (time_scheme.cpp:133-135)
+//   k_face_flux<d>   WENO-5 face fluxes along axis d, one thread per face
+//                    (Weno5::x/y/z_sweep, Weno5cw::*_sweep)
+//   k_update         flux differences + centered viscous terms + RK combination
+//                    (Weno5::compute_residual, CenteredDiffusion::compute_residual,
+//                    TimeScheme::substep)
+// Per step: k_step_begin (dt reduction over W, then U = cons(W), U0 = U).
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+
+#include "ns_common.cuh"
+#include "ns_kernels.h"
+
+namespace nsb {
+
+// ---------------------------------------------------------------------------
+// equation of state (src/eq_of_state.cpp:32-87)
+
+__device__ __forceinline__ void prim_from_cons(const double u[5], double gm1, double w[5]) {
+    double ir = 1.0 / u[0];
+    w[0] = u[0];
+    w[2] = u[2] * ir;
+    w[3] = u[3] * ir;
+    w[4] = u[4] * ir;
+    double kin = 0.5 * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
+    w[1] = gm1 * (u[1] - u[0] * kin);
+}
+
+__device__ __forceinline__ void cons_from_prim(const double w[5], double inv_gm1, double u[5]) {
+    u[0] = w[0];
+    u[2] = w[0] * w[2];
+    u[3] = w[0] * w[3];
+    u[4] = w[0] * w[4];
+    double kin = 0.5 * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
+    u[1] = w[1] * inv_gm1 + kin;
+}
+
+// EqOfState::local_dt (src/eq_of_state.cpp:89-101), min over directions
+__device__ __forceinline__ double local_dt(const double w[5], const Consts& c) {
+    double cs = sqrt(c.gamma * w[1] / w[0]);
+    double ex = c.dx / fmax(fabs(w[2] + cs), fabs(w[2] - cs));
+    double ey = c.dy / fmax(fabs(w[3] + cs), fabs(w[3] - cs));
+    double ez = c.dz / fmax(fabs(w[4] + cs), fabs(w[4] - cs));
+    double t = (ey < ex) ? ey : ex;
+    return (ez < t) ? ez : t;
+}
+
+__device__ __forceinline__ double local_dt_physical(const double w[5], const Consts& c) {
+    double cs = sqrt(c.gamma * w[1] / w[0]);
+    double r = (fabs(w[2]) + cs) * c.inv_dx + (fabs(w[3]) + cs) * c.inv_dy;
+    if (c.dim == 3) r += (fabs(w[4]) + cs) * c.inv_dz;
+    return 1.0 / r;
+}
+
+// block-wide min of a positive double, then one 64-bit atomicMin on its bit
+// pattern (positive IEEE doubles order like their unsigned bit patterns)
+__device__ __forceinline__ void block_min_to(double v, unsigned long long* slot) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
+    int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
+    int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        v = lane < nw ? red[lane] : INFINITY;
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0 && v < INFINITY)
+            atomicMin(slot, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// step begin: dt from W at the step start (TimeScheme::set_dt), then
+// U = cons(W) on every cell (time_scheme.cpp:124) and U0 = U (:126).
+// FROM_U: the state is U after the previous step; W = prim(U) first
+// (time_scheme.cpp:69).  Grid: (ceil(NZp/32), ceil(NY/4), NX).
+
+template <bool FROM_U, bool PHYS>
+__global__ void __launch_bounds__(128) k_step_begin(double* __restrict__ W, double* __restrict__ U,
+                                                    double* __restrict__ U0, Box b, Consts c,
+                                                    unsigned long long* __restrict__ slot) {
+    int kh = blockIdx.x * 32 + threadIdx.x;
+    int jh = blockIdx.y * 4 + threadIdx.y;
+    int ih = blockIdx.z;
+    double best = INFINITY;
+    if (kh < b.nz + 2 * NG && jh < b.NY) {
+        long long o = b.at(ih, jh, kh);
+        double w[5], u[5];
+        if (FROM_U) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) u[q] = U[q * b.fstride + o];
+            prim_from_cons(u, c.gm1, w);
+#pragma unroll
+            for (int q = 0; q < 5; q++) W[q * b.fstride + o] = w[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; q++) w[q] = W[q * b.fstride + o];
+        }
+        bool interior = ih >= NG && ih < b.nx + NG && jh >= NG && jh < b.ny + NG && kh >= NG &&
+                        kh < b.nz + NG;
+        if (interior) {
+            double dt = PHYS ? local_dt_physical(w, c) : local_dt(w, c);
+            if (dt < best) best = dt;  // NaN never lowers the minimum (time_scheme.cpp:117)
+        }
+        cons_from_prim(w, c.inv_gm1, u);
+#pragma unroll
+        for (int q = 0; q < 5; q++) U[q * b.fstride + o] = u[q];
+        if (interior) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u[q];
+        }
+    }
+    block_min_to(best, slot);
+}
+
+// W = prim(U) on every cell (end of TimeScheme::step, time_scheme.cpp:69)
+__global__ void __launch_bounds__(128) k_prim_all(double* __restrict__ W, const double* __restrict__ U,
+                                                  Box b, Consts c) {
+    int kh = blockIdx.x * 32 + threadIdx.x;
+    int jh = blockIdx.y * 4 + threadIdx.y;
+    int ih = blockIdx.z;
+    if (kh >= b.nz + 2 * NG || jh >= b.NY) return;
+    long long o = b.at(ih, jh, kh);
+    double u[5], w[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) u[q] = U[q * b.fstride + o];
+    prim_from_cons(u, c.gm1, w);
+#pragma unroll
+    for (int q = 0; q < 5; q++) W[q * b.fstride + o] = w[q];
+}
+
+// U = cons(W) on every cell
+__global__ void __launch_bounds__(128) k_cons_all(const double* __restrict__ W, double* __restrict__ U,
+                                                  Box b, Consts c) {
+    int kh = blockIdx.x * 32 + threadIdx.x;
+    int jh = blockIdx.y * 4 + threadIdx.y;
+    int ih = blockIdx.z;
+    if (kh >= b.nz + 2 * NG || jh >= b.NY) return;
+    long long o = b.at(ih, jh, kh);
+    double u[5], w[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) w[q] = W[q * b.fstride + o];
+    cons_from_prim(w, c.inv_gm1, u);
+#pragma unroll
+    for (int q = 0; q < 5; q++) U[q * b.fstride + o] = u[q];
+}
+
+// CFL minimum over the interior of W (TimeScheme::get_local_max_dt, time_scheme.cpp:98-125)
+template <bool PHYS>
+__global__ void __launch_bounds__(128) k_min_dt(const double* __restrict__ W, Box b, Consts c,
+                                                unsigned long long* __restrict__ slot) {
+    int k = blockIdx.x * 32 + threadIdx.x;
+    int j = blockIdx.y * 4 + threadIdx.y;
+    int i = blockIdx.z;
+    double best = INFINITY;
+    if (k < b.nz && j < b.ny) {
+        long long o = b.at(i + NG, j + NG, k + NG);
+        double w[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) w[q] = W[q * b.fstride + o];
+        double dt = PHYS ? local_dt_physical(w, c) : local_dt(w, c);
+        if (dt < best) best = dt;
+    }
+    block_min_to(best, slot);
+}
+
+// ---------------------------------------------------------------------------
+// stage prologue: Neumann copy / periodic wrap of U on the face halos
+// (boundary_neumann.cpp:22-132, communicator.cpp:6-143: face regions only),
+// then W = prim(U) on every cell (eq_of_state.cpp:61-87).
+
+__global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, double* __restrict__ U,
+                                                   Box b, Consts c) {
+    int kh = blockIdx.x * 32 + threadIdx.x;
+    int jh = blockIdx.y * 4 + threadIdx.y;
+    int ih = blockIdx.z;
+    if (kh >= b.nz + 2 * NG || jh >= b.NY) return;
+    int i = ih - NG, j = jh - NG, k = kh - NG;
+    bool ox = i < 0 || i >= b.nx, oy = j < 0 || j >= b.ny, oz = k < 0 || k >= b.nz;
+    long long o = b.at(ih, jh, kh);
+    double u[5], w[5];
+    if ((int)ox + (int)oy + (int)oz == 1) {
+        int si = ox ? fold(i, b.nx, c.periodic[0]) : i;
+        int sj = oy ? fold(j, b.ny, c.periodic[1]) : j;
+        int sk = oz ? fold(k, b.nz, c.periodic[2]) : k;
+        long long s = b.at(si + NG, sj + NG, sk + NG);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            u[q] = U[q * b.fstride + s];
+            U[q * b.fstride + o] = u[q];
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < 5; q++) u[q] = U[q * b.fstride + o];
+    }
+    prim_from_cons(u, c.gm1, w);
+#pragma unroll
+    for (int q = 0; q < 5; q++) W[q * b.fstride + o] = w[q];
+}
+
+// ---------------------------------------------------------------------------
+// WENO-5 face fluxes
+
+// Tangent frame of ConvectionFlux::orthogonal_unit_vectors (convection_flux.cpp:63-115)
+// for the axis normals: x: l = e_z, m = -e_y;  y: l = e_z, m = e_x;  z: l = -e_y, m = e_x.
+template <int DIR>
+struct Frame;
+template <>
+struct Frame<0> {
+    static constexpr int l_ax = 2, l_sg = 1, m_ax = 1, m_sg = -1;
+};
+template <>
+struct Frame<1> {
+    static constexpr int l_ax = 2, l_sg = 1, m_ax = 0, m_sg = 1;
+};
+template <>
+struct Frame<2> {
+    static constexpr int l_ax = 1, l_sg = -1, m_ax = 0, m_sg = 1;
+};
+
+// State index of textbook component t of [rho, rho u, rho v, rho w, rho E].
+// The reference applies its textbook-ordered eigenvectors to the state order
+// [rho, rhoE, rhou, rhov, rhow] unchanged (convection_flux.cpp:153-171 vs
+// src/domain.hpp:52), i.e. the identity map; the physical form permutes.
+template <bool PHYS>
+__device__ __forceinline__ constexpr int st(int t) {
+    return PHYS ? (t == 0 ? 0 : (t == 4 ? 1 : t + 1)) : t;
+}
+
+template <typename T>
+__device__ __forceinline__ T tsqrt(T x) {
+    if constexpr (sizeof(T) == 8) return sqrt(x); else return sqrtf(x);
+}
+template <typename T>
+__device__ __forceinline__ T trcp(T x) {
+    if constexpr (sizeof(T) == 8) return 1.0 / x; else return __frcp_rn(x);
+}
+
+// Left/right eigenvectors of the 3D Euler Jacobian (ConvectionFlux::eigenvectors,
+// convection_flux.cpp:117-175) at the arithmetic face average, kept as the
+// scalars the sparse rows need.
+template <typename T>
+struct Eig {
+    T vel[3], qn, ql, qm, q2, c, c2, H, Kpc, K2pc, inv2c;
+};
+
+template <int DIR, bool PHYS, typename T>
+__device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma) {
+    Eig<T> e;
+    T rho = wa[0], p = wa[1];
+    e.vel[0] = wa[2]; e.vel[1] = wa[3]; e.vel[2] = wa[4];
+    e.qn = e.vel[DIR];
+    e.ql = Frame<DIR>::l_sg * e.vel[Frame<DIR>::l_ax];
+    e.qm = Frame<DIR>::m_sg * e.vel[Frame<DIR>::m_ax];
+    e.q2 = e.vel[0] * e.vel[0] + e.vel[1] * e.vel[1] + e.vel[2] * e.vel[2];
+    // reference: c2 = gamma/(p rho) (convection_flux.cpp:139)
+    e.c2 = PHYS ? gamma * p * trcp(rho) : gamma * trcp(p * rho);
+    e.c = tsqrt(e.c2);
+    T K = gamma - T(1);
+    e.H = e.c2 * trcp(K) + T(0.5) * e.q2;
+    e.Kpc = K * trcp(T(2) * e.c2);
+    e.K2pc = T(2) * e.Kpc;  // K/c2
+    e.inv2c = trcp(T(2) * e.c);
+    return e;
+}
+
+// char_r = sum_t L[r][t] f[st(t)] for the textbook rows of L
+template <int DIR, bool PHYS, int R, typename T>
+__device__ __forceinline__ T lproj(const Eig<T>& e, const T f[5]) {
+    const T f0 = f[st<PHYS>(0)];
+    const T fe = f[st<PHYS>(4)];
+    const T fm[3] = {f[st<PHYS>(1)], f[st<PHYS>(2)], f[st<PHYS>(3)]};
+    if constexpr (R == 1) {  // (-qm, m, 0)
+        constexpr int a = Frame<DIR>::m_ax;
+        return -e.qm * f0 + (Frame<DIR>::m_sg > 0 ? fm[a] : -fm[a]);
+    } else if constexpr (R == 4) {  // (-ql, l, 0)
+        constexpr int a = Frame<DIR>::l_ax;
+        return -e.ql * f0 + (Frame<DIR>::l_sg > 0 ? fm[a] : -fm[a]);
+    } else if constexpr (R == 2) {  // (1 - Kpc q2, K u/c2, K v/c2, K w/c2, -K/c2)
+        return (T(1) - e.Kpc * e.q2) * f0 + e.K2pc * (e.vel[0] * fm[0] + e.vel[1] * fm[1] + e.vel[2] * fm[2]) -
+               e.K2pc * fe;
+    } else {  // R == 0 (+) or R == 3 (-): (Kpc q2/2 +- qn/2c, -(Kpc u +- n_x/2c), ..., Kpc)
+        constexpr T sg = (R == 0) ? T(1) : T(-1);
+        T s = (T(0.5) * e.Kpc * e.q2 + sg * e.qn * e.inv2c) * f0 -
+              e.Kpc * (e.vel[0] * fm[0] + e.vel[1] * fm[1] + e.vel[2] * fm[2]) + e.Kpc * fe;
+        return s - sg * e.inv2c * fm[DIR];
+    }
+}
+
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
+__global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
+                                                   const double* __restrict__ U, Box b, Consts c,
+                                                   TF* __restrict__ F, FaceBox fb) {
+    int kk = blockIdx.x * 32 + threadIdx.x;
+    int bb = blockIdx.y * 4 + threadIdx.y;
+    int aa = blockIdx.z;
+    if (kk >= fb.n2 || bb >= fb.n1) return;
+    // halo'd index of stencil cell 0 (cell a-2 for the face between a and a+1)
+    int ih = aa + (DIR == 0 ? 0 : NG), jh = bb + (DIR == 1 ? 0 : NG), kh = kk + (DIR == 2 ? 0 : NG);
+    long long o0 = b.at(ih, jh, kh);
+    const long long step = DIR == 0 ? (long long)b.NY * b.NZp : (DIR == 1 ? b.NZp : 1);
+    const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1), half = T(0.5);
+
+    T fL[5][5], fR[5][5];  // [variable][stencil]
+    T wa[5];
+    T alpha = T(3);  // ConvectionFlux::max_eigenvalue returns 3.0 everywhere (convection_flux.cpp:241)
+    T Fc[6][5], Uc[6][5];
+    (void)Fc; (void)Uc;
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        long long o = o0 + s * step;
+        T w[5], u[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            w[q] = T(W[q * b.fstride + o]);
+            u[q] = T(U[q * b.fstride + o]);
+        }
+        if constexpr (CHAR) {
+            if (s == 2) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) wa[q] = w[q];
+            }
+            if (s == 3) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + w[q]);
+            }
+        }
+        // Euler flux along DIR (ConvectionFlux::form_flux, convection_flux.cpp:23-61)
+        T rho = w[0], p = w[1];
+        T qn = w[2 + DIR];
+        T c2 = gamma * p * trcp(rho);
+        T H = c2 * inv_gm1 + half * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
+        T rq = rho * qn;
+        T f[5];
+        f[0] = rq;
+        f[1] = rq * H;
+        f[2] = rq * w[2] + (DIR == 0 ? p : T(0));
+        f[3] = rq * w[3] + (DIR == 1 ? p : T(0));
+        f[4] = rq * w[4] + (DIR == 2 ? p : T(0));
+        if constexpr (PHYS) {
+            // local Lax-Friedrichs speed max(|qn|+c) over the 6-cell stencil
+            T a = fabs(qn) + tsqrt(c2);
+            alpha = (s == 0) ? a : (a > alpha ? a : alpha);
+#pragma unroll
+            for (int q = 0; q < 5; q++) { Fc[s][q] = f[q]; Uc[s][q] = u[q]; }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                if (s <= 4) fL[q][s] = (f[q] + alpha * u[q]) * half;
+                if (s >= 1) fR[q][s - 1] = (f[q] - alpha * u[q]) * half;
+            }
+        }
+    }
+    if constexpr (PHYS) {
+#pragma unroll
+        for (int s = 0; s < 6; s++)
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                if (s <= 4) fL[q][s] = (Fc[s][q] + alpha * Uc[s][q]) * half;
+                if (s >= 1) fR[q][s - 1] = (Fc[s][q] - alpha * Uc[s][q]) * half;
+            }
+    }
+
+    T out[5];
+    if constexpr (!CHAR) {
+#pragma unroll
+        for (int q = 0; q < 5; q++)
+            out[q] = weno_left<T, BORGES>(fL[q][0], fL[q][1], fL[q][2], fL[q][3], fL[q][4]) +
+                     weno_right<T, BORGES>(fR[q][0], fR[q][1], fR[q][2], fR[q][3], fR[q][4]);
+    } else {
+        Eig<T> e = make_eig<DIR, PHYS, T>(wa, gamma);
+        T ft[5];
+        // characteristic projection L fL, L fR per stencil column, WENO per field
+        // (Weno5cw::compute_num_flux, weno-5cw.cpp:4-28)
+#define NS_CHAR_FIELD(RR)                                                        \
+        {                                                                        \
+            T cl[5], cr[5];                                                      \
+            _Pragma("unroll") for (int s = 0; s < 5; s++) {                      \
+                T vl[5] = {fL[0][s], fL[1][s], fL[2][s], fL[3][s], fL[4][s]};    \
+                T vr[5] = {fR[0][s], fR[1][s], fR[2][s], fR[3][s], fR[4][s]};    \
+                cl[s] = lproj<DIR, PHYS, RR, T>(e, vl);                          \
+                cr[s] = lproj<DIR, PHYS, RR, T>(e, vr);                          \
+            }                                                                    \
+            ft[RR] = weno_left<T, BORGES>(cl[0], cl[1], cl[2], cl[3], cl[4]) +   \
+                     weno_right<T, BORGES>(cr[0], cr[1], cr[2], cr[3], cr[4]);   \
+        }
+        NS_CHAR_FIELD(0)
+        NS_CHAR_FIELD(1)
+        NS_CHAR_FIELD(2)
+        NS_CHAR_FIELD(3)
+        NS_CHAR_FIELD(4)
+#undef NS_CHAR_FIELD
+        // back-projection R ft; textbook rows of R (convection_flux.cpp:153-158)
+        T acc = ft[0] + ft[2] + ft[3];
+        T tb[5];
+        tb[0] = acc;
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            T cn = (a == DIR) ? e.c : T(0);
+            T v = e.vel[a] * acc - cn * ft[0] + cn * ft[3];
+            if (a == Frame<DIR>::m_ax) v += (Frame<DIR>::m_sg > 0 ? ft[1] : -ft[1]);
+            if (a == Frame<DIR>::l_ax) v += (Frame<DIR>::l_sg > 0 ? ft[4] : -ft[4]);
+            tb[1 + a] = v;
+        }
+        tb[4] = e.H * (ft[0] + ft[3]) + e.qn * e.c * (ft[3] - ft[0]) + e.qm * ft[1] +
+                half * e.q2 * ft[2] + e.ql * ft[4];
+#pragma unroll
+        for (int t = 0; t < 5; t++) out[st<PHYS>(t)] = tb[t];
+    }
+    long long fo = fb.at(aa, bb, kk);
+#pragma unroll
+    for (int q = 0; q < 5; q++) F[q * fb.fstride + fo] = TF(out[q]);
+}
+
+// ---------------------------------------------------------------------------
+// centered viscous terms, reference semantics (CenteredDiffusion::compute_residual,
+// src/diffusion_schemes/centered_diffusion.cpp:70-182 with the stress helpers of
+// diffusion_scheme.cpp:3-58; dmu = 0 terms dropped, which is exact).
+//   - d2/dy2 applies the x-stencil scaled by 1/dy^2 (cd-n.cpp:77)
+//   - Tauyy = tauxx (:143); the x work term uses Tauxy*dv_dy (:148);
+//     the y heat-flux term multiplies by 1 where the pressure belongs (:166)
+//   - 2D terms only; rhoW untouched (:173-176)
+//   - mixed derivatives differentiate first derivatives that are zero outside
+//     the interior along a non-periodic axis (derivative halos are only filled
+//     by the periodic exchange, :22-24)
+
+template <int H, typename TV>
+__device__ __forceinline__ void viscous_reference(const double* __restrict__ W, const Box& b,
+                                                  const Consts& c, int i, int j, int k, TV r[5]) {
+    const long long fs = b.fstride;
+    const long long sx = (long long)b.NY * b.NZp, sy = b.NZp;
+    const long long o = b.at(i + NG, j + NG, k + NG);
+    TV cx1[2 * H + 1], cy1[2 * H + 1], cxx[2 * H + 1], cyy[2 * H + 1];
+#pragma unroll
+    for (int t = 0; t <= 2 * H; t++) {
+        cx1[t] = TV(c.df[3 - H + t] * c.inv_dx);
+        cy1[t] = TV(c.df[3 - H + t] * c.inv_dy);
+        cxx[t] = TV(c.ddf[3 - H + t] * c.inv_dx * c.inv_dx);
+        cyy[t] = TV(c.ddf[3 - H + t] * c.inv_dy * c.inv_dy);
+    }
+    // first and second derivatives of rho, p, u, v at the cell
+    TV Dx[4], Dy[4], Dxx[4], Dyy[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        TV sx1 = 0, sy1 = 0, sxx = 0, syy = 0;
+#pragma unroll
+        for (int t = 0; t <= 2 * H; t++) {
+            TV wx = TV(W[q * fs + o + (t - H) * sx]);
+            TV wy = TV(W[q * fs + o + (t - H) * sy]);
+            if (t != H) { sx1 += wx * cx1[t]; sy1 += wy * cy1[t]; }
+            sxx += wx * cxx[t];
+            syy += wx * cyy[t];
+        }
+        Dx[q] = sx1; Dy[q] = sy1; Dxx[q] = sxx; Dyy[q] = syy;
+    }
+    // mixed derivatives of u (q=2) and v (q=3)
+    TV Dxy[2], Dyx[2];
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+        const int q = 2 + v;
+        TV sxy = 0, syx = 0;
+#pragma unroll
+        for (int s = 0; s <= 2 * H; s++) {
+            if (s == H) continue;
+            // d/dy of (d/dx W) at row j+s-H
+            int jj = j + s - H;
+            if ((jj >= 0 && jj < b.ny) || c.periodic[1]) {
+                int jw = fold(jj, b.ny, 1);
+                long long ob = b.at(i + NG, jw + NG, k + NG);
+                TV dx = 0;
+#pragma unroll
+                for (int t = 0; t <= 2 * H; t++)
+                    if (t != H) dx += TV(W[q * fs + ob + (t - H) * sx]) * cx1[t];
+                sxy += dx * cy1[s];
+            }
+            // d/dx of (d/dy W) at column i+s-H
+            int ii = i + s - H;
+            if ((ii >= 0 && ii < b.nx) || c.periodic[0]) {
+                int iw = fold(ii, b.nx, 1);
+                long long ob = b.at(iw + NG, j + NG, k + NG);
+                TV dy = 0;
+#pragma unroll
+                for (int t = 0; t <= 2 * H; t++)
+                    if (t != H) dy += TV(W[q * fs + ob + (t - H) * sy]) * cy1[t];
+                syx += dy * cx1[s];
+            }
+        }
+        Dxy[v] = sxy; Dyx[v] = syx;
+    }
+    const TV mu = TV(c.mu), lamb = TV(c.lamb), two = TV(2);
+    const TV Uc = TV(W[2 * fs + o]), Vc = TV(W[3 * fs + o]), P = TV(W[1 * fs + o]),
+             RHO = TV(W[o]);
+    const TV du_dx = Dx[2], du_dy = Dy[2], du_dxdx = Dxx[2], du_dydy = Dyy[2];
+    const TV du_dxdy = Dxy[0], du_dydx = Dyx[0];
+    const TV dv_dy = Dy[3], dv_dx = Dx[3], dv_dxdx = Dxx[3], dv_dydy = Dyy[3];
+    const TV dv_dydx = Dyx[1], dv_dxdy = Dxy[1];
+    const TV drho_dx = Dx[0], dp_dx = Dx[1], drho_dxdx = Dxx[0], dp_dxdx = Dxx[1];
+    const TV drho_dy = Dy[0], dp_dy = Dy[1], drho_dydy = Dyy[0], dp_dydy = Dyy[1];
+
+    TV Dtauxx_dx = two * mu * du_dxdx + lamb * (du_dxdx + dv_dydx);
+    TV Dtauyy_dy = two * mu * dv_dydy + lamb * (du_dxdy + dv_dydy);
+    TV Dtauxy_dx = mu * (du_dydx + dv_dxdx);
+    TV Dtauyx_dy = mu * (du_dydy + dv_dxdy);
+    TV Tauxx = two * mu * du_dx + lamb * (du_dx + dv_dy);
+    TV Tauyy = Tauxx;
+    TV Tauxy = mu * (du_dy + dv_dx);
+    TV Dtauvx_dx = Uc * Dtauxx_dx + Vc * Dtauxy_dx + Tauxx * du_dx + Tauxy * dv_dy;
+    TV Dtauvy_dy = Uc * Dtauyx_dy + Vc * Dtauyy_dy + Tauyy * dv_dy + Tauxy * du_dy;
+    TV ir = TV(1) / RHO, ir2 = ir * ir, ir3 = ir2 * ir;
+    TV heat = TV(c.heat);
+    TV Dqx_dx = -heat * (mu * (two * ir2 * drho_dx * dp_dx + ir * dp_dxdx + ir3 * P * drho_dx * drho_dx -
+                               ir2 * P * drho_dxdx));
+    TV Dqy_dy = -heat * (mu * (two * ir2 * drho_dy * dp_dy + ir * dp_dydy + ir3 * drho_dy * drho_dy -
+                               ir2 * P * drho_dydy));
+    r[1] += -Dtauvx_dx - Dtauvy_dy + Dqx_dx + Dqy_dy;
+    r[2] += -Dtauxx_dx - Dtauyx_dy;
+    r[3] += -Dtauyy_dy - Dtauxy_dx;
+}
+
+// Physical semantics: full 3D viscous stress and heat flux with constant mu
+// (no reference counterpart).  Mixed derivatives read the boundary-filled W,
+// folding corner/edge cells back into the filled region.
+template <int H, typename TV>
+__device__ __forceinline__ void viscous_physical(const double* __restrict__ W, const Box& b,
+                                                 const Consts& c, int i, int j, int k, TV r[5]) {
+    const long long fs = b.fstride;
+    const long long st3[3] = {(long long)b.NY * b.NZp, (long long)b.NZp, 1};
+    const long long o = b.at(i + NG, j + NG, k + NG);
+    const int nd = c.dim == 3 ? 3 : 2;
+    const double inv[3] = {c.inv_dx, c.inv_dy, c.inv_dz};
+    TV gu[3][3] = {}, lap[3] = {}, gT[3] = {}, lapT = 0, gdiv[3] = {};
+    for (int bx = 0; bx < nd; bx++) {
+#pragma unroll
+        for (int t = 0; t <= 2 * H; t++) {
+            long long oo = o + (t - H) * st3[bx];
+            TV c1 = TV(c.df[3 - H + t] * inv[bx]);
+            TV c2 = TV(c.ddf[3 - H + t] * inv[bx] * inv[bx]);
+            TV T = TV(W[1 * fs + oo]) / TV(W[oo]);
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                TV va = TV(W[(2 + a) * fs + oo]);
+                gu[a][bx] += va * c1;
+                lap[a] += va * c2;
+                if (a == bx) gdiv[a] += va * c2;
+            }
+            gT[bx] += T * c1;
+            lapT += T * c2;
+        }
+    }
+    const int n3[3] = {b.nx, b.ny, b.nz};
+    const int c3[3] = {i, j, k};
+    for (int a = 0; a < nd; a++)
+        for (int bx = 0; bx < nd; bx++) {
+            if (a == bx) continue;
+            TV acc = 0;
+#pragma unroll
+            for (int s = 0; s <= 2 * H; s++)
+#pragma unroll
+                for (int t = 0; t <= 2 * H; t++) {
+                    int cc[3] = {c3[0], c3[1], c3[2]};
+                    cc[a] += s - H;
+                    cc[bx] += t - H;
+                    // corner/edge cells are not filled: fold along both axes
+                    cc[a] = fold(cc[a], n3[a], c.periodic[a]);
+                    cc[bx] = fold(cc[bx], n3[bx], c.periodic[bx]);
+                    long long oo = b.at(cc[0] + NG, cc[1] + NG, cc[2] + NG);
+                    acc += TV(W[(2 + bx) * fs + oo]) * TV(c.df[3 - H + s] * inv[a]) *
+                           TV(c.df[3 - H + t] * inv[bx]);
+                }
+            gdiv[a] += acc;
+        }
+    const TV mu = TV(c.mu), lamb = TV(c.lamb);
+    TV uv[3] = {TV(W[2 * fs + o]), TV(W[3 * fs + o]), TV(W[4 * fs + o])};
+    TV div = gu[0][0] + gu[1][1] + gu[2][2];
+    TV work = 0, diss = 0, mom[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        mom[a] = mu * lap[a] + (mu + lamb) * gdiv[a];
+        work += uv[a] * mom[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int bx = 0; bx < 3; bx++) {
+            TV tab = mu * (gu[a][bx] + gu[bx][a]) + (a == bx ? lamb * div : TV(0));
+            diss += tab * gu[a][bx];
+        }
+    (void)gT;
+    r[2] -= mom[0];
+    r[3] -= mom[1];
+    r[4] -= mom[2];
+    r[1] -= work + diss + TV(c.heat) * mu * lapT;
+}
+
+// ---------------------------------------------------------------------------
+// cell update: R = sum_d (f_d(+) - f_d(-))/d  (+ viscous), then
+//   MODE_STAGE: U = U0*m1 + U*m2 + R*(mc*dt)    (TimeScheme::substep, time_scheme.cpp:72-96)
+//   MODE_RHS  : Rout += R
+// dt = CFL * min(1e10, reduced minimum) (time_scheme.cpp:98-136).
+
+template <int MODE, int H, bool PHYS, typename TF, typename TV>
+__global__ void __launch_bounds__(128) k_update(const double* __restrict__ W, double* __restrict__ U,
+                                                const double* __restrict__ U0,
+                                                const TF* __restrict__ Fx, const TF* __restrict__ Fy,
+                                                const TF* __restrict__ Fz, Box b, FaceBox fx,
+                                                FaceBox fy, FaceBox fz, Consts c, int flags,
+                                                const unsigned long long* __restrict__ slot,
+                                                double m1, double m2, double mc,
+                                                double* __restrict__ Rout, double* __restrict__ clock) {
+    int k = blockIdx.x * 32 + threadIdx.x;
+    int j = blockIdx.y * 4 + threadIdx.y;
+    int i = blockIdx.z;
+    if (k >= b.nz || j >= b.ny) return;
+    double r[5] = {0, 0, 0, 0, 0};
+    if (flags & UPD_CONV) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            r[q] += (double(Fx[q * fx.fstride + fx.at(i + 1, j, k)]) -
+                     double(Fx[q * fx.fstride + fx.at(i, j, k)])) * c.inv_dx;
+            r[q] += (double(Fy[q * fy.fstride + fy.at(i, j + 1, k)]) -
+                     double(Fy[q * fy.fstride + fy.at(i, j, k)])) * c.inv_dy;
+            if (flags & UPD_CONVZ)
+                r[q] += (double(Fz[q * fz.fstride + fz.at(i, j, k + 1)]) -
+                         double(Fz[q * fz.fstride + fz.at(i, j, k)])) * c.inv_dz;
+        }
+    }
+    if constexpr (H > 0) {
+        TV rv[5] = {0, 0, 0, 0, 0};
+        if constexpr (PHYS)
+            viscous_physical<H, TV>(W, b, c, i, j, k, rv);
+        else
+            viscous_reference<H, TV>(W, b, c, i, j, k, rv);
+#pragma unroll
+        for (int q = 1; q < 5; q++) r[q] += double(rv[q]);
+    }
+    long long o = b.at(i + NG, j + NG, k + NG);
+    if constexpr (MODE == MODE_STAGE) {
+        double mn = __longlong_as_double((long long)*slot);
+        double dt = fmin(1e10, mn) * c.cfl;
+        double m3 = mc * dt;
+        if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) {
+            clock[0] = dt;
+            clock[1] += dt;
+        }
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            long long a = q * b.fstride + o;
+            U[a] = (U0[a] * m1) + (U[a] * m2) + (r[q] * m3);
+        }
+    } else {
+        if (flags & UPD_OVERWRITE) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) Rout[q * b.fstride + o] = r[q];
+        } else {
+#pragma unroll
+            for (int q = 0; q < 5; q++) Rout[q * b.fstride + o] += r[q];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host <-> device layout transposes (reference AoS [i][j][k][q], unpadded
+// (nx+6)(ny+6)(nz+6) x 5  <->  device SoA planes)
+
+__global__ void __launch_bounds__(128) k_aos_to_soa(const double* __restrict__ A, double* __restrict__ S,
+                                                    Box b) {
+    int kh = blockIdx.x * 32 + threadIdx.x;
+    int jh = blockIdx.y * 4 + threadIdx.y;
+    int ih = blockIdx.z;
+    int NZ = b.nz + 2 * NG;
+    if (kh >= NZ || jh >= b.NY) return;
+    long long a = (((long long)ih * b.NY + jh) * NZ + kh) * 5;
+    long long o = b.at(ih, jh, kh);
+#pragma unroll
+    for (int q = 0; q < 5; q++) S[q * b.fstride + o] = A[a + q];
+}
+
+__global__ void __launch_bounds__(128) k_soa_to_aos(const double* __restrict__ S, double* __restrict__ A,
+                                                    Box b) {
+    int kh = blockIdx.x * 32 + threadIdx.x;
+    int jh = blockIdx.y * 4 + threadIdx.y;
+    int ih = blockIdx.z;
+    int NZ = b.nz + 2 * NG;
+    if (kh >= NZ || jh >= b.NY) return;
+    long long a = (((long long)ih * b.NY + jh) * NZ + kh) * 5;
+    long long o = b.at(ih, jh, kh);
+#pragma unroll
+    for (int q = 0; q < 5; q++) A[a + q] = S[q * b.fstride + o];
+}
+
+// ---------------------------------------------------------------------------
+// global diagnostics over the interior (FP64): sums of conserved variables,
+// kinetic energy, enstrophy (second-order central curl), non-finite count.
+__global__ void __launch_bounds__(128) k_diagnostics(const double* __restrict__ U, Box b, Consts c,
+                                                     double* __restrict__ acc) {
+    int k = blockIdx.x * 32 + threadIdx.x;
+    int j = blockIdx.y * 4 + threadIdx.y;
+    int i = blockIdx.z;
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (k < b.nz && j < b.ny) {
+        long long o = b.at(i + NG, j + NG, k + NG);
+        double u[5];
+        bool bad = false;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            u[q] = U[q * b.fstride + o];
+            bad |= !isfinite(u[q]);
+        }
+        double dV = c.dx * c.dy * c.dz;
+        v[0] = u[0] * dV;
+        v[1] = u[2] * dV;
+        v[2] = u[3] * dV;
+        v[3] = u[4] * dV;
+        v[4] = u[1] * dV;
+        v[5] = 0.5 * (u[2] * u[2] + u[3] * u[3] + u[4] * u[4]) / u[0] * dV;
+        // velocity of neighbours through the periodic/clamped index map
+        auto vel = [&](int ii, int jj, int kk, int a) {
+            ii = fold(ii, b.nx, c.periodic[0]);
+            jj = fold(jj, b.ny, c.periodic[1]);
+            kk = fold(kk, b.nz, c.periodic[2]);
+            long long oo = b.at(ii + NG, jj + NG, kk + NG);
+            return U[(2 + a) * b.fstride + oo] / U[oo];
+        };
+        double dwdy = (vel(i, j + 1, k, 2) - vel(i, j - 1, k, 2)) * 0.5 * c.inv_dy;
+        double dvdz = (vel(i, j, k + 1, 1) - vel(i, j, k - 1, 1)) * 0.5 * c.inv_dz;
+        double dudz = (vel(i, j, k + 1, 0) - vel(i, j, k - 1, 0)) * 0.5 * c.inv_dz;
+        double dwdx = (vel(i + 1, j, k, 2) - vel(i - 1, j, k, 2)) * 0.5 * c.inv_dx;
+        double dvdx = (vel(i + 1, j, k, 1) - vel(i - 1, j, k, 1)) * 0.5 * c.inv_dx;
+        double dudy = (vel(i, j + 1, k, 0) - vel(i, j - 1, k, 0)) * 0.5 * c.inv_dy;
+        double wx = dwdy - dvdz, wy = dudz - dwdx, wz = dvdx - dudy;
+        v[6] = 0.5 * u[0] * (wx * wx + wy * wy + wz * wz) * dV;
+        v[7] = bad ? 1.0 : 0.0;
+    }
+    __shared__ double red[8][4];
+    int warp = threadIdx.y;  // blockDim = (32,4): one warp per row
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        double x = v[m];
+        for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+        if (threadIdx.x == 0) red[m][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.y == 0 && threadIdx.x < 8) {
+        int m = threadIdx.x;
+        atomicAdd(&acc[m], red[m][0] + red[m][1] + red[m][2] + red[m][3]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+
+static dim3 cell_grid(const Box& b) {  // all halo'd cells
+    return dim3((b.nz + 2 * NG + 31) / 32, (b.NY + 3) / 4, b.NX);
+}
+static dim3 interior_grid(const Box& b) {
+    return dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx);
+}
+
+void launch_step_begin(bool from_u, bool phys, double* W, double* U, double* U0, const Box& b,
+                       const Consts& c, unsigned long long* slot, cudaStream_t s) {
+    dim3 blk(32, 4);
+    if (from_u) {
+        if (phys) k_step_begin<true, true><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
+        else k_step_begin<true, false><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
+    } else {
+        if (phys) k_step_begin<false, true><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
+        else k_step_begin<false, false><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
+    }
+}
+
+void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s) {
+    k_prim_all<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c);
+}
+
+void launch_cons_all(const double* W, double* U, const Box& b, const Consts& c, cudaStream_t s) {
+    k_cons_all<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c);
+}
+
+void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, unsigned long long* slot,
+                   cudaStream_t s) {
+    if (phys) k_min_dt<true><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, slot);
+    else k_min_dt<false><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, slot);
+}
+
+void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s) {
+    k_fill_prim<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c);
+}
+
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
+static void face_one(const double* W, const double* U, const Box& b, const Consts& c, void* F,
+                     const FaceBox& fb, cudaStream_t s) {
+    dim3 grid((fb.n2 + 31) / 32, (fb.n1 + 3) / 4, fb.n0);
+    k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
+}
+
+template <int DIR, typename T, typename TF>
+static void face_dispatch(bool chr, bool borges, bool phys, const double* W, const double* U,
+                          const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s) {
+    if (chr) {
+        if (borges) {
+            if (phys) face_one<DIR, true, true, true, T, TF>(W, U, b, c, F, fb, s);
+            else face_one<DIR, true, true, false, T, TF>(W, U, b, c, F, fb, s);
+        } else {
+            if (phys) face_one<DIR, true, false, true, T, TF>(W, U, b, c, F, fb, s);
+            else face_one<DIR, true, false, false, T, TF>(W, U, b, c, F, fb, s);
+        }
+    } else {
+        if (borges) {
+            if (phys) face_one<DIR, false, true, true, T, TF>(W, U, b, c, F, fb, s);
+            else face_one<DIR, false, true, false, T, TF>(W, U, b, c, F, fb, s);
+        } else {
+            if (phys) face_one<DIR, false, false, true, T, TF>(W, U, b, c, F, fb, s);
+            else face_one<DIR, false, false, false, T, TF>(W, U, b, c, F, fb, s);
+        }
+    }
+}
+
+void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
+                      const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
+                      cudaStream_t s) {
+    if (fp32) {
+        if (dir == 0) face_dispatch<0, float, float>(chr, borges, phys, W, U, b, c, F, fb, s);
+        else if (dir == 1) face_dispatch<1, float, float>(chr, borges, phys, W, U, b, c, F, fb, s);
+        else face_dispatch<2, float, float>(chr, borges, phys, W, U, b, c, F, fb, s);
+    } else {
+        if (dir == 0) face_dispatch<0, double, double>(chr, borges, phys, W, U, b, c, F, fb, s);
+        else if (dir == 1) face_dispatch<1, double, double>(chr, borges, phys, W, U, b, c, F, fb, s);
+        else face_dispatch<2, double, double>(chr, borges, phys, W, U, b, c, F, fb, s);
+    }
+}
+
+template <int MODE, int H, bool PHYS, typename TF, typename TV>
+static void update_one(const UpdateArgs& a, cudaStream_t s) {
+    k_update<MODE, H, PHYS, TF, TV><<<interior_grid(a.b), dim3(32, 4), 0, s>>>(
+        a.W, a.U, a.U0, (const TF*)a.F[0], (const TF*)a.F[1], (const TF*)a.F[2], a.b, a.fb[0],
+        a.fb[1], a.fb[2], a.c, a.flags, a.slot, a.m1, a.m2, a.mc, a.Rout, a.clock);
+}
+
+template <int MODE, bool PHYS, typename TF, typename TV>
+static void update_h(int h, const UpdateArgs& a, cudaStream_t s) {
+    switch (h) {
+        case 0: update_one<MODE, 0, PHYS, TF, TV>(a, s); break;
+        case 1: update_one<MODE, 1, PHYS, TF, TV>(a, s); break;
+        case 2: update_one<MODE, 2, PHYS, TF, TV>(a, s); break;
+        default: update_one<MODE, 3, PHYS, TF, TV>(a, s); break;
+    }
+}
+
+template <int MODE>
+static void update_mode(const UpdateArgs& a, cudaStream_t s) {
+    int h = a.viscous ? a.c.order / 2 : 0;
+    if (a.fp32) {
+        if (a.phys) update_h<MODE, true, float, float>(h, a, s);
+        else update_h<MODE, false, float, float>(h, a, s);
+    } else {
+        if (a.phys) update_h<MODE, true, double, double>(h, a, s);
+        else update_h<MODE, false, double, double>(h, a, s);
+    }
+}
+
+void launch_update(const UpdateArgs& a, cudaStream_t s) {
+    if (a.mode == MODE_STAGE) update_mode<MODE_STAGE>(a, s);
+    else update_mode<MODE_RHS>(a, s);
+}
+
+void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s) {
+    k_aos_to_soa<<<cell_grid(b), dim3(32, 4), 0, s>>>(A, S, b);
+}
+void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s) {
+    k_soa_to_aos<<<cell_grid(b), dim3(32, 4), 0, s>>>(S, A, b);
+}
+void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* acc, cudaStream_t s) {
+    k_diagnostics<<<interior_grid(b), dim3(32, 4), 0, s>>>(U, b, c, acc);
+}
+
+}  // namespace nsb

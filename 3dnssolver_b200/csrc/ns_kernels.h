@@ -1,0 +1,47 @@
+// ns_kernels.h -- host-side launchers of the device kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ns_common.cuh"
+
+namespace nsb {
+
+enum { MODE_STAGE = 0, MODE_RHS = 1 };
+enum { UPD_CONV = 1, UPD_CONVZ = 2, UPD_OVERWRITE = 4 };
+
+struct UpdateArgs {
+    const double* W;
+    double* U;
+    const double* U0;
+    const void* F[3];
+    Box b;
+    FaceBox fb[3];
+    Consts c;
+    int flags;       // UPD_*
+    int mode;        // MODE_*
+    bool viscous;
+    bool phys;
+    bool fp32;
+    const unsigned long long* slot;  // reduced CFL minimum of this step
+    double m1, m2, mc;               // U = U0*m1 + U*m2 + R*(mc*dt)
+    double* Rout;                    // MODE_RHS target (halo'd SoA)
+    double* clock;                   // [last dt, accumulated time], updated once per step (nullable)
+};
+
+void launch_step_begin(bool from_u, bool phys, double* W, double* U, double* U0, const Box& b,
+                       const Consts& c, unsigned long long* slot, cudaStream_t s);
+void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s);
+void launch_cons_all(const double* W, double* U, const Box& b, const Consts& c, cudaStream_t s);
+void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, unsigned long long* slot,
+                   cudaStream_t s);
+void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s);
+void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
+                      const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
+                      cudaStream_t s);
+void launch_update(const UpdateArgs& a, cudaStream_t s);
+void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s);
+void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s);
+void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* acc, cudaStream_t s);
+
+}  // namespace nsb

@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit RHS + SSP-RK3 time step on B200.
+
+Metric: cell-updates/s per RK3 stage = nx*ny*nz*3*steps / seconds.
+Workload (one "step" = one TimeScheme::step, i.e. three RK stages):
+  temporal double shear layer, 256^3 periodic cells on [0,2pi]^3, rho=1,
+  p=1/(gamma M^2) with M=0.5, seeded SplitMix64 noise 1e-3 on v and w,
+  FP64 characteristic-wise WENO-5 (Shu weights, Lax-Friedrichs splitting) +
+  second-order centered viscous terms (mu = 6.283e-4, Pr = 0.72), CFL 0.5,
+  reference semantics.  Synthetic input; the device state (2.9 GB) is larger
+  than L2, so no flush is needed between timed steps.
+
+Arms:
+  default            our CUDA path (libns_b200.so through its C ABI)
+  --impl reference   the reference's own CPU TimeScheme::step (compiled from its
+                     sources into oracle/_ref, OpenMP on all host cores)
+Multi-GPU (torchrun): every rank advances an independent replica (the path is
+single-GPU by design: no collective on the data path); value sums the ranks,
+time is the max over ranks.
+"""
+import argparse
+import csv
+import importlib
+import io
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per RK3 stage on 1 B200 (FP32+learned vs plain FP64) at stated L2 err"
+UNIT = "cell-updates/s"
+
+FORMS = {
+    # name: (convection, precision, sensor, dtype label)
+    "fp64_char": (2, 0, 0, "f64"),
+    "fp64_comp": (1, 0, 0, "f64"),
+    "fp32_char": (2, 1, 0, "f32 (f64 RK3 accumulation and reductions)"),
+    "fp32_sensor": (2, 1, 1, "f32 + bf16 sensor (f64 RK3 accumulation and reductions)"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="cells per axis of the shear-layer box")
+    ap.add_argument("--form", default="fp64_char", choices=sorted(FORMS))
+    ap.add_argument("--also", default="fp64_comp,fp32_char",
+                    help="extra forms timed after the headline (comma list, '' for none)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_params(pkg, n, form):
+    conv, prec, sensor, _ = FORMS[form]
+    L = 2 * math.pi
+    # mu = rho0 * dU * delta / Re with dU = 2, delta = 0.05*2pi, Re = 1000
+    return pkg.make_params(n, n, n, L=(L, L, L), mu=2.0 * 0.05 * 2 * math.pi / 1000.0, Pr=0.72,
+                           gamma=1.4, cfl=0.5, convection=conv, diffusion_order=2, precision=prec,
+                           sensor=sensor)
+
+
+def workload_name(n, form):
+    return (f"shear_layer {n}^3 periodic [0,2pi]^3 M=0.5 Re=1000, {form} WENO-5 (Shu, LF alpha=3) "
+            f"+ CD-2 viscous, SSP-RK3 CFL 0.5, reference semantics")
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv",
+                                          "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = list(csv.reader(io.StringIO(self.tmp.read())))
+        os.unlink(self.tmp.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows[1:]:
+            if len(r) < 9 or r[0].strip() != str(self.gpu):
+                continue
+            try:
+                sm.append(float(r[1].split()[0]))
+                smax = float(r[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own TimeScheme::step (oracle/_ref) on host cores
+
+def cpu_baseline(steps=2, warmup=1, n=256):
+    from oracle import oracle as O
+    pkg = importlib.import_module("3dnssolver_b200")
+    threads = os.cpu_count() or 1
+    p = workload_params(pkg, n, "fp64_char")
+    if O.ref_available(strict=False):
+        r = O.ref_bench(p, steps=steps, warmup=warmup, threads=threads, timed=True)
+        return {"value": r["cell_updates_per_s"], "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{steps} timed TimeScheme::step calls (after {warmup} warm-up) of the "
+                          f"same workload at {n}^3, reference sources built with -O3 -ffast-math, "
+                          f"OpenMP {threads} threads, 1 rank", "seconds": r["seconds"]}
+    # the oracle port (strict IEEE C restatement) when the reference build is absent
+    wl = importlib.import_module("3dnssolver_b200.workloads")
+    n = 64
+    p = workload_params(pkg, n, "fp64_char")
+    W = wl.shear_layer(p, seed=1)
+    O.run(p, W, 1)
+    t0 = time.perf_counter()
+    O.run(p, W, steps)
+    sec = time.perf_counter() - t0
+    return {"value": n ** 3 * 3 * steps / sec, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} steps at {n}^3 of the oracle port", "seconds": sec}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    # sample grid: keep the whole --warmup/--steps run within a few minutes
+    n = 256 if args.warmup + args.steps <= 16 else 128
+    try:
+        from oracle import oracle as O
+        if not O.ref_available(strict=False):
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "oracle/_ref/ref_harness_timed not built (needs the reference tree)"}))
+            return 0
+        pkg = importlib.import_module("3dnssolver_b200")
+        p = workload_params(pkg, n, "fp64_char")
+        threads = os.cpu_count() or 1
+        r = O.ref_bench(p, steps=args.steps, warmup=args.warmup, threads=threads, timed=True)
+    except Exception as e:  # report, do not crash the driver
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"}))
+        return 0
+    v = r["cell_updates_per_s"]
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * r["seconds"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name(args.n, "fp64_char"), "sample_grid": [n, n, n],
+                   "parallelism": "1 rank, OpenMP"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"each step one TimeScheme::step at {n}^3 (reference sources, "
+                                   f"-O3 -ffast-math, OpenMP {threads} threads)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    pkg = importlib.import_module("3dnssolver_b200")
+    wl = importlib.import_module("3dnssolver_b200.workloads")
+    n = args.n
+    cells = n ** 3
+    p = workload_params(pkg, n, args.form)
+    W0 = wl.shear_layer(p, seed=1 + rank)
+    stream = torch.cuda.current_stream()
+
+    def time_form(form, steps, warmup, sample_clocks=False):
+        pf = workload_params(pkg, n, form)
+        s = pkg.Solver(pf)
+        s.set_stream(stream.cuda_stream)
+        s.upload_primitive(W0)
+        s.advance(warmup)
+        torch.cuda.synchronize()
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.start()
+        barrier()
+        torch.cuda.synchronize()
+        l0 = s.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.advance(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        launches = s.launches - l0
+        clocks = clk.stop() if clk else None
+        diag = s.diagnostics()
+        return s, ms, launches, clocks, diag
+
+    s, ms, launches, clocks, diag = time_form(args.form, args.steps, args.warmup, sample_clocks=True)
+    ms_max = max_over_ranks(ms)
+    value = world * cells * 3 * args.steps / (ms_max / 1000.0)
+
+    # per-kernel device times of one step (events between kernels on the same stream)
+    profs = [s.profile_step() for _ in range(3)]
+    prof = {k: statistics.mean(pr[k] for pr in profs) for k in profs[0]}
+    faces_ms = {k: v for k, v in prof.items() if k.startswith("face_")}
+    dom = max(prof, key=prof.get)
+    # algorithmic bytes: a face-flux launch reads W and U (2 x 5 doubles per cell) and
+    # writes 5 doubles per face; an update launch reads U, U0 and 3 face arrays and writes U
+    elem = 4 if FORMS[args.form][1] == 1 else 8
+    fx_faces = (n + 1) * n * n
+    face_bytes = cells * 80 + fx_faces * 5 * elem
+    upd_bytes = cells * (3 * 40) + 3 * fx_faces * 5 * elem + cells * 40
+    alg = {"face_x": face_bytes, "face_y": face_bytes, "face_z": face_bytes, "update": upd_bytes,
+           "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120}
+    per_launch_ms = prof[dom] / (1 if dom == "step_begin" else 3)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": f"k_face_flux ({dom}, {args.form})" if dom.startswith("face")
+                else dom, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": alg[dom], "launch_ms": round(per_launch_ms, 4),
+                "note": "FP64 characteristic-wise WENO is FP64-pipe bound; see compute_roofline"}
+
+    # end to end through the C ABI with host buffers: ns_time_step uploads W from pinned
+    # host memory, runs the step and downloads W every step
+    Wh_t = torch.empty(W0.shape, dtype=torch.float64, pin_memory=True)
+    Wh = Wh_t.numpy()
+    Wh[...] = W0
+    s.time_step(Wh)  # warm-up
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        s.time_step(Wh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": world * cells * 3 * args.e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Wh.nbytes),
+           "steps": args.e2e_steps, "api": "ns_time_step (TimeScheme::step drop-in), pinned host W"}
+    s.close()
+
+    # extra forms on the same workload (same timing rules)
+    forms = {args.form: {"value": value, "ms_per_step": ms_max / args.steps}}
+    for f in [x for x in args.also.split(",") if x and x != args.form]:
+        try:
+            s2, ms2, _, _, _ = time_form(f, args.steps, args.warmup)
+            s2.close()
+            ms2 = max_over_ranks(ms2)
+            forms[f] = {"value": world * cells * 3 * args.steps / (ms2 / 1000.0),
+                        "ms_per_step": ms2 / args.steps}
+        except Exception as e:
+            forms[f] = {"error": str(e)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(n=n)
+        except Exception as e:
+            cpu = {"error": str(e)}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": FORMS[args.form][3], "data": "synthetic",
+            "config": {"workload": workload_name(n, args.form), "grid": [n, n, n], "form": args.form,
+                       "l2": "no flush: device state 2.9 GB > 126 MB L2",
+                       "parallelism": f"{world} independent replica(s), no data-path collective"},
+            "roofline": roofline,
+            "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "forms": forms,
+            "diagnostics": {"nonfinite": diag["nonfinite"], "dt": diag["dt"],
+                            "mass": diag["mass"], "kinetic": diag["kinetic"]},
+        }
+        print(json.dumps(out))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -27,6 +27,12 @@
 extern "C" {
 #endif
 
+#if defined(__GNUC__)
+#define NS_API __attribute__((visibility("default")))
+#else
+#define NS_API
+#endif
+
 #define NS_ABI_VERSION 1
 #define NS_NGC 3 /* ghost cells per side, src/params.hpp:16-18 */
 #define NS_NQ 5  /* variables per cell, src/domain.cpp:160 */
@@ -97,61 +103,68 @@ typedef struct ns_diagnostics {
 
 typedef struct ns_ctx ns_ctx;
 
-const char* ns_status_string(ns_status s);
+NS_API const char* ns_status_string(ns_status s);
 /* Message of the last failure on this thread ("" if none). */
-const char* ns_last_error_string(void);
-int ns_abi_version(void);
+NS_API const char* ns_last_error_string(void);
+NS_API int ns_abi_version(void);
 
 /* Fills *p with the defaults of the tutorial case (src/io/reader.cpp:3-172 fields). */
-ns_status ns_params_default(ns_params* p);
+NS_API ns_status ns_params_default(ns_params* p);
 
 /* Creates a context and allocates its device state on the current CUDA device.
  * Replaces Driver::run's construction of Grid/Domain/operators
  * (src/driver.cpp:9-25) for the hot path. */
-ns_status ns_create(const ns_params* p, ns_ctx** out);
-void ns_destroy(ns_ctx* ctx);
+NS_API ns_status ns_create(const ns_params* p, ns_ctx** out);
+NS_API void ns_destroy(ns_ctx* ctx);
 /* Adopts a caller's cudaStream_t (NULL selects the context's own stream). */
-ns_status ns_set_stream(ns_ctx* ctx, void* cuda_stream);
+NS_API ns_status ns_set_stream(ns_ctx* ctx, void* cuda_stream);
 /* Number of elements of one host halo'd array: (nx+6)(ny+6)(nz+6)*5. */
-size_t ns_host_array_elems(const ns_params* p);
+NS_API size_t ns_host_array_elems(const ns_params* p);
 
 /* ---- state transfer (host AoS with halos) -------------------------------- */
 /* Sets the primitive state W (Domain::get_NS_primitive_array, src/domain.hpp:36). */
-ns_status ns_upload_primitive(ns_ctx* ctx, const double* W);
-ns_status ns_download_primitive(ns_ctx* ctx, double* W);
-ns_status ns_download_conservative(ns_ctx* ctx, double* U);
+NS_API ns_status ns_upload_primitive(ns_ctx* ctx, const double* W);
+NS_API ns_status ns_download_primitive(ns_ctx* ctx, double* W);
+NS_API ns_status ns_download_conservative(ns_ctx* ctx, double* U);
 
 /* ---- operator plug-ins (drop-in for the reference virtual interfaces) ----- */
 /* ConvectionScheme::solve(grid, W, U, R) (src/convection_schemes/convection_scheme.hpp:26,
  * Weno5::solve src/convection_schemes/weno-5.cpp:3-37): R += convective residual.
  * W and U are read including their halos as given; only R's interior is written. */
-ns_status ns_convection_solve(ns_ctx* ctx, const double* W, const double* U, double* R);
+NS_API ns_status ns_convection_solve(ns_ctx* ctx, const double* W, const double* U, double* R);
 /* DiffusionScheme::solve(grid, comm, W, R) (src/diffusion_schemes/diffusion_scheme.hpp:14-17,
  * CenteredDiffusion::solve src/diffusion_schemes/centered_diffusion.cpp:3-68): R += viscous residual.
  * W is read including its halos as given. */
-ns_status ns_diffusion_solve(ns_ctx* ctx, const double* W, double* R);
+NS_API ns_status ns_diffusion_solve(ns_ctx* ctx, const double* W, double* R);
 /* First RK stage's right-hand side from a primitive field: prim->cons on all cells,
  * boundary fill + halo exchange, cons->prim, R = 0, then the selected terms
  * (src/time_scheme.cpp:124-140).  W is read (halos included), R's interior written. */
-ns_status ns_rhs(ns_ctx* ctx, const double* W, double* R, int terms);
+NS_API ns_status ns_rhs(ns_ctx* ctx, const double* W, double* R, int terms);
 /* TimeScheme::set_dt (src/time_scheme.cpp:98-136): CFL * min over interior cells. */
-ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out);
+NS_API ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out);
 /* TimeScheme::step (src/time_scheme.hpp:25-29, src/time_scheme.cpp:3-70): one SSP-RK3
  * step of host W (in/out) and U (out, may be NULL); dt_out receives the step's dt.
  * Host <-> device copies are part of the call. */
-ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out);
+NS_API ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out);
 
 /* ---- device-resident time loop -------------------------------------------- */
 /* Runs nsteps steps of TimeScheme::step on the device-resident state (the Driver
  * loop, src/driver.cpp:43-68, without host copies).  Asynchronous on the
  * context's stream; no host synchronisation inside. */
-ns_status ns_advance(ns_ctx* ctx, int nsteps);
+NS_API ns_status ns_advance(ns_ctx* ctx, int nsteps);
 /* Blocks until the context's stream is idle; NS_ERR_NONFINITE if
  * check_finite was requested and the state holds NaN/Inf. */
-ns_status ns_synchronize(ns_ctx* ctx);
-ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
+NS_API ns_status ns_synchronize(ns_ctx* ctx);
+NS_API ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
+/* Kernel classes timed by ns_profile_step */
+enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FACE_Y = 3,
+       NS_PROF_FACE_Z = 4, NS_PROF_UPDATE = 5, NS_PROF_N = 6 };
+/* Runs one time step of the device-resident state with CUDA events recorded
+ * between its kernels on the context's stream; ms[c] receives the device time
+ * of kernel class c summed over the step (n >= NS_PROF_N). */
+NS_API ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n);
 /* Device kernels launched by this context since creation (for launch accounting). */
-long long ns_kernel_launches(ns_ctx* ctx);
+NS_API long long ns_kernel_launches(ns_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,195 @@
+"""GPU parity of the CUDA path (through the C ABI) against the oracle and the
+golden fixtures made by the reference.
+
+Tolerance: 1e-12 relative L2 per conserved field (the FP64 bar of the reference
+path); the kernels use fused multiply-adds and single-division WENO weights, so
+they agree with the reference arithmetic to rounding, not bit-for-bit.
+"""
+import importlib
+
+import numpy as np
+import pytest
+
+from conftest import interior, load_golden, rel_l2
+
+pkg = importlib.import_module("3dnssolver_b200")
+wl = importlib.import_module("3dnssolver_b200.workloads")
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+P, N = pkg.BC_PERIODIC, pkg.BC_NEUMANN
+Z, META = load_golden()
+
+
+def _golden_params(kw):
+    return pkg.make_params(*META["shape"], mu=0.02, Pr=0.72, gamma=1.4, L=(1.0, 0.9, 0.8), **kw)
+
+
+def _assert_close(a, b, tol=TOL, what=""):
+    err = rel_l2(interior(a), interior(b)) if a.ndim == 4 and a.shape[0] > 6 else rel_l2(a, b)
+    assert np.isfinite(a).all() if a.ndim != 4 else np.isfinite(interior(a)).all()
+    assert (err <= tol).all(), f"{what}: rel L2 per field {err}"
+    return err
+
+
+@pytest.mark.parametrize("case", META["cases"], ids=[c["name"] for c in META["cases"]])
+def test_gpu_matches_reference_golden(case):
+    p = _golden_params(case["params"])
+    W = Z[case["name"] + "/W"]
+    with pkg.Solver(p) as s:
+        if case["kind"] == "rhs":
+            R = s.rhs(W, terms=case["n"])
+            err = rel_l2(interior(R), Z[case["name"] + "/R"])
+            assert (err <= TOL).all(), err
+        else:
+            Wg = W.copy()
+            Ug = s.new_array()
+            dts = [s.time_step(Wg, Ug) for _ in range(case["n"])]
+            np.testing.assert_allclose(dts, Z[case["name"] + "/dt"], rtol=1e-14, atol=0)
+            assert (rel_l2(interior(Wg), Z[case["name"] + "/Wn"]) <= TOL).all()
+            assert (rel_l2(interior(Ug), Z[case["name"] + "/Un"]) <= TOL).all()
+
+
+RHS_CASES = [
+    # (shape, conv, weights, order, bc, dim, smooth)
+    ((12, 10, 8), 1, 0, 2, (P, P, P), 3, True),
+    ((12, 10, 8), 1, 1, 4, (N, P, N), 3, False),
+    ((12, 10, 8), 2, 0, 6, (P, N, P), 3, False),
+    ((12, 10, 8), 2, 1, 2, (N, N, N), 3, False),
+    ((16, 7, 9), 2, 0, 4, (P, P, P), 3, True),
+    ((5, 6, 7), 2, 0, 2, (N, P, P), 3, False),
+    ((3, 3, 3), 1, 0, 2, (P, P, P), 3, False),
+    ((3, 4, 3), 2, 1, 6, (N, N, N), 3, False),
+    ((9, 11, 1), 2, 0, 2, (P, P, P), 2, False),
+    ((33, 6, 40), 2, 0, 2, (P, N, P), 3, False),
+]
+
+
+@pytest.mark.parametrize("shape,conv,weights,order,bc,dim,smooth", RHS_CASES)
+@pytest.mark.parametrize("terms", [1, 2, 3])
+def test_rhs_matches_oracle(oracle, shape, conv, weights, order, bc, dim, smooth, terms):
+    p = pkg.make_params(*shape, dim=dim, convection=conv, weights=weights, diffusion_order=order, bc=bc,
+                        mu=0.03, L=(1.0, 1.3, 0.7))
+    W = wl.random_field(p, seed=hash((shape, conv, order)) % 1000, smooth=smooth)
+    with pkg.Solver(p) as s:
+        R = s.rhs(W, terms=terms)
+    Ro = oracle.rhs(p, W, terms=terms)
+    err = rel_l2(interior(R), interior(Ro))
+    # rhoW has no viscous term; with convection off its residual is exactly zero
+    ok = np.where(np.sqrt((interior(Ro) ** 2).reshape(-1, 5).sum(0)) == 0,
+                  np.abs(interior(R)).reshape(-1, 5).max(0) == 0, err <= TOL)
+    assert ok.all(), f"rel L2 per field {err}"
+
+
+@pytest.mark.parametrize("conv", [1, 2])
+def test_operator_solves_use_caller_halos(oracle, conv):
+    """ns_convection_solve / ns_diffusion_solve read the caller's halos verbatim and accumulate."""
+    p = pkg.make_params(10, 9, 8, convection=conv, diffusion_order=4, bc=(N, P, P), mu=0.05)
+    W0 = wl.random_field(p, seed=5, smooth=False)
+    W, U = oracle.prologue(p, W0)
+    rng = np.random.default_rng(0)
+    R0 = rng.standard_normal(W.shape)  # accumulate onto a nonzero residual, halos included
+    with pkg.Solver(p) as s:
+        Rc = s.convection_solve(W, U, R0.copy())
+        Rd = s.diffusion_solve(W, R0.copy())
+    Rco = oracle.convection_solve(p, W, U, R0)
+    Rdo = oracle.diffusion_solve(p, W, R0)
+    _assert_close(Rc - R0, Rco - R0, what="convection")
+    _assert_close(Rd[..., :4] - R0[..., :4], Rdo[..., :4] - R0[..., :4], what="diffusion")
+    g = 3
+    np.testing.assert_array_equal(Rc[:g], R0[:g])  # halos untouched
+    np.testing.assert_array_equal(Rd[..., 4], R0[..., 4])  # rhoW untouched by the viscous terms
+
+
+@pytest.mark.parametrize("conv,order,bc,weights", [
+    (1, 2, (P, P, P), 0), (2, 4, (N, P, P), 0), (2, 6, (N, N, N), 1), (1, 6, (P, N, P), 1),
+])
+def test_time_steps_match_oracle(oracle, conv, order, bc, weights):
+    p = pkg.make_params(14, 12, 10, convection=conv, diffusion_order=order, bc=bc, weights=weights,
+                        mu=0.02, cfl=0.3)
+    W0 = wl.random_field(p, seed=9, smooth=True)
+    Wo, Uo, dto = oracle.run(p, W0, 4)
+    with pkg.Solver(p) as s:
+        Wg, Ug = W0.copy(), s.new_array()
+        dts = [s.time_step(Wg, Ug) for _ in range(4)]
+    np.testing.assert_allclose(dts, dto, rtol=1e-13)
+    _assert_close(Wg, Wo, what="W")
+    _assert_close(Ug, Uo, what="U")
+
+
+def test_device_resident_advance_equals_host_steps(oracle):
+    p = pkg.make_params(16, 16, 16, convection=2, diffusion_order=2, bc=(P, P, P), mu=0.01, cfl=0.4)
+    W0 = wl.random_field(p, seed=3, smooth=True)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(5)
+        Wd = s.download_primitive()
+        Ud = s.download_conservative()
+        diag = s.diagnostics()
+    with pkg.Solver(p) as s:
+        Wh, Uh = W0.copy(), s.new_array()
+        dts = [s.time_step(Wh, Uh) for _ in range(5)]
+    np.testing.assert_array_equal(interior(Wd), interior(Wh))
+    np.testing.assert_array_equal(interior(Ud), interior(Uh))
+    assert diag["steps"] == 5
+    assert diag["dt"] == dts[-1]
+    np.testing.assert_allclose(diag["time"], sum(dts), rtol=1e-14)
+    Wo, Uo, dto = oracle.run(p, W0, 5)
+    _assert_close(Wd, Wo, what="W after 5 steps")
+
+
+def test_compute_dt_matches_reference(oracle):
+    p = pkg.make_params(12, 9, 7, L=(2.0, 1.0, 0.5), cfl=0.45)
+    W = wl.random_field(p, seed=2, smooth=False)
+    with pkg.Solver(p) as s:
+        dt = s.compute_dt(W)
+    assert dt == pytest.approx(oracle.compute_dt(p, W), rel=1e-15)
+
+
+def test_conservation_periodic_inviscid():
+    """Flux-form update: mass and energy are conserved to rounding on a periodic box."""
+    p = pkg.make_params(24, 20, 16, convection=2, diffusion=pkg.DIFF_NONE, mu=0.0, cfl=0.4)
+    W0 = wl.random_field(p, seed=4, smooth=False)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        d0 = s.diagnostics()
+        s.advance(10)
+        d1 = s.diagnostics()
+    assert not d1["nonfinite"]
+    assert abs(d1["mass"] - d0["mass"]) <= 1e-13 * abs(d0["mass"])
+    assert abs(d1["energy"] - d0["energy"]) <= 1e-13 * abs(d0["energy"])
+
+
+def test_shear_layer_trajectory_component_wise(oracle):
+    """Multi-step trajectory on the shear-layer workload (component-wise WENO, CD-2)."""
+    import math
+    p = pkg.make_params(32, 32, 32, L=(2 * math.pi,) * 3, mu=6.283e-4, Pr=0.72, cfl=0.5,
+                        convection=pkg.CONV_WENO5, diffusion_order=2)
+    W0 = wl.shear_layer(p, seed=1)
+    n = 20
+    Wo, Uo, dto = oracle.run(p, W0, n)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(n)
+        Ug = s.download_conservative()
+    err = rel_l2(interior(Ug), interior(Uo))
+    # rhoW is noise-amplitude: judge it against the momentum magnitude
+    mag = np.sqrt((interior(Uo)[..., 2:5] ** 2).sum())
+    err_w = np.sqrt(((interior(Ug)[..., 4] - interior(Uo)[..., 4]) ** 2).sum()) / mag
+    assert (err[:4] <= TOL).all(), err
+    assert err_w <= TOL, err_w
+
+
+def test_fp32_form_close_to_fp64(oracle):
+    p64 = pkg.make_params(24, 24, 24, convection=2, diffusion_order=2, mu=0.01, cfl=0.4)
+    p32 = pkg.make_params(24, 24, 24, convection=2, diffusion_order=2, mu=0.01, cfl=0.4,
+                          precision=pkg.PREC_FP32)
+    W0 = wl.random_field(p64, seed=8, smooth=True)
+    Wo, Uo, _ = oracle.run(p64, W0, 3)
+    with pkg.Solver(p32) as s:
+        s.upload_primitive(W0)
+        s.advance(3)
+        U32 = s.download_conservative()
+    err = rel_l2(interior(U32), interior(Uo))
+    assert (err[[0, 1]] <= 1e-5).all(), err
+    assert (err <= 1e-3).all(), err
