@@ -229,7 +229,9 @@ def main():
     cells = n ** 3
     p = workload_params(pkg, n, args.form)
     W0 = wl.shear_layer(p, seed=1 + rank)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the context adopts it, so CUDA events recorded on it bracket
+    # exactly the library's kernels (torch's default stream is the legacy NULL stream)
+    stream = torch.cuda.Stream()
 
     def time_form(form, steps, warmup, sample_clocks=False):
         pf = workload_params(pkg, n, form)

@@ -116,7 +116,8 @@ NS_API ns_status ns_params_default(ns_params* p);
  * (src/driver.cpp:9-25) for the hot path. */
 NS_API ns_status ns_create(const ns_params* p, ns_ctx** out);
 NS_API void ns_destroy(ns_ctx* ctx);
-/* Adopts a caller's cudaStream_t (NULL selects the context's own stream). */
+/* Adopts a caller's cudaStream_t.  NULL selects the context's own non-blocking
+ * stream again (the legacy default stream cannot be adopted). */
 NS_API ns_status ns_set_stream(ns_ctx* ctx, void* cuda_stream);
 /* Number of elements of one host halo'd array: (nx+6)(ny+6)(nz+6)*5. */
 NS_API size_t ns_host_array_elems(const ns_params* p);
