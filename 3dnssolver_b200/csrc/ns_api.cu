@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -622,3 +623,113 @@ ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
 long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 }  // extern "C"
+
+// ===========================================================================
+// Convection residual without any device allocation.
+//
+// For callers that must not allocate device memory themselves or have it
+// allocated on their behalf: host programs that hand out all device memory
+// from their own pool and give a plugin no allocation budget, and control or
+// real-time loops that cannot afford cudaMalloc's latency, its implicit device
+// synchronisation or an out-of-memory failure in the middle of a run.  The
+// caller supplies the inputs and the output in device memory; the face fluxes
+// that the other entry points keep in context-owned buffers live here in one
+// fixed array compiled into the library.
+//
+// Cost and limits: the array takes NS_NOALLOC_SCRATCH_BYTES (32 MiB) on every
+// GPU that loads this library, for the life of the process.  A grid fits when
+// the face fluxes of all convected axes fit in it (FP64: 5 doubles per face;
+// about 64^3 cells in 3D); larger grids are rejected with NS_ERR_INVALID_ARG.
+// All calls on a device share the array, so calls whose kernels overlap on
+// that GPU (different streams, or several host threads) race and corrupt each
+// other's results; serialise them.  Every scratch element a call reads is
+// written earlier in the same call, so nothing needs clearing between calls.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = NS_NOALLOC_SCRATCH_BYTES;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The symbol's
+// host-side name is only a stand-in, so its address is looked up once per
+// device with that device current (the first call on each device).
+ns_status noalloc_scratch(void** out) {
+    int dev = -1;
+    NS_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(NS_ERR_UNSUPPORTED, "device ordinal %d is beyond the %d devices supported", dev,
+                    kNoAllocMaxDevices);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(NS_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
+                        cudaGetErrorString(e));
+        g_noalloc_addr[dev] = ptr;
+    }
+    *out = g_noalloc_addr[dev];
+    return NS_OK;
+}
+
+}  // namespace
+
+extern "C" ns_status ns_convection_solve_noalloc(const ns_params* p, const double* W,
+                                                 const double* U, double* R, void* stream) {
+    NS_TRY(validate(p));
+    if (!W || !U || !R) return fail(NS_ERR_INVALID_ARG, "W, U and R must be non-NULL device pointers");
+    if (p->convection == NS_CONV_NONE)
+        return fail(NS_ERR_INVALID_ARG, "convection is NS_CONV_NONE: there is no residual to compute");
+    if (p->sensor) return fail(NS_ERR_UNSUPPORTED, "the sensor-gated form needs a context (ns_create)");
+    // the caller's layout: 5 planes of the halo'd box, unpadded, k fastest
+    Box b;
+    b.nx = p->nx; b.ny = p->ny; b.nz = p->nz;
+    b.NX = p->nx + 2 * NS_NGC; b.NY = p->ny + 2 * NS_NGC; b.NZp = p->nz + 2 * NS_NGC;
+    b.fstride = (long long)b.NX * b.NY * b.NZp;
+    FaceBox fb[3];
+    for (int d = 0; d < 3; d++) fb[d] = make_facebox(p->nx, p->ny, p->nz, d);
+    const int nd = p->dim == 3 ? 3 : 2;
+    const bool f32 = p->precision == NS_PREC_FP32;
+    const size_t elem = f32 ? sizeof(float) : sizeof(double);
+    size_t need = 0;
+    for (int d = 0; d < nd; d++) need += (size_t)NS_NQ * (size_t)fb[d].fstride * elem;
+    if (need > kNoAllocScratchBytes)
+        return fail(NS_ERR_INVALID_ARG,
+                    "grid %dx%dx%d needs %zu bytes of face-flux scratch; the no-allocation entry point "
+                    "holds %zu bytes (about 64^3 cells in FP64)",
+                    p->nx, p->ny, p->nz, need, kNoAllocScratchBytes);
+    void* base = nullptr;
+    NS_TRY(noalloc_scratch(&base));
+    const Consts c = make_consts(p);
+    cudaStream_t s = (cudaStream_t)stream;
+    void* F[3] = {nullptr, nullptr, nullptr};
+    char* cur = (char*)base;
+    for (int d = 0; d < nd; d++) {
+        F[d] = cur;
+        cur += (size_t)NS_NQ * (size_t)fb[d].fstride * elem;
+    }
+    const bool chr = p->convection == NS_CONV_WENO5_CHAR;
+    const bool borges = p->weights == NS_WEIGHTS_BORGES;
+    const bool ph = p->semantics == NS_SEM_PHYSICAL;
+    for (int d = 0; d < nd; d++) launch_face_flux(d, chr, borges, ph, f32, W, U, b, c, F[d], fb[d], s);
+    UpdateArgs a;
+    memset(&a, 0, sizeof a);
+    a.W = W;
+    for (int d = 0; d < 3; d++) { a.F[d] = F[d]; a.fb[d] = fb[d]; }
+    a.b = b;
+    a.c = c;
+    a.flags = UPD_CONV | (p->dim == 3 ? UPD_CONVZ : 0);
+    a.mode = MODE_RHS;
+    a.viscous = false;
+    a.phys = ph;
+    a.fp32 = f32;
+    a.Rout = R;
+    launch_update(a, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(NS_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return NS_OK;
+}

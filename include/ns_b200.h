@@ -164,6 +164,27 @@ enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FAC
  * between its kernels on the context's stream; ms[c] receives the device time
  * of kernel class c summed over the step (n >= NS_PROF_N). */
 NS_API ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n);
+/* ---- convection residual without device allocation -------------------------
+ * No counterpart in the reference.  For callers that may not allocate device
+ * memory or have it allocated for them: hosts that serve all device memory
+ * from their own pool and give a plugin no allocation budget, and real-time
+ * loops that cannot take cudaMalloc's latency, its device synchronisation or
+ * an out-of-memory failure mid-run.  Same result as ns_convection_solve
+ * (R += convective residual, halos of W and U read as given) but W, U and R
+ * are DEVICE pointers, each to 5 consecutive planes (q = 0..4) of the halo'd
+ * box (nx+6) x (ny+6) x (nz+6) doubles with k fastest; work is queued on
+ * cuda_stream (NULL: the legacy default stream) and the call returns without
+ * waiting.  The face fluxes live in one array of NS_NOALLOC_SCRATCH_BYTES
+ * compiled into the library, held on every GPU that loads it until the
+ * process exits; grids whose face fluxes do not fit (beyond about 64^3 cells
+ * in FP64) are rejected with NS_ERR_INVALID_ARG.  The first call on each
+ * device looks up that array's device address; make that first call before
+ * any stream capture begins.  All calls on a device share the array: calls
+ * that overlap on the GPU race, so serialise them.  Nothing is allocated:
+ * no cudaMalloc, no cudaFree, no allocating library call. */
+#define NS_NOALLOC_SCRATCH_BYTES (32u << 20)
+NS_API ns_status ns_convection_solve_noalloc(const ns_params* p, const double* W, const double* U,
+                                             double* R, void* cuda_stream);
 /* Device kernels launched by this context since creation (for launch accounting). */
 NS_API long long ns_kernel_launches(ns_ctx* ctx);
 
