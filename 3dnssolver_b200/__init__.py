@@ -21,7 +21,8 @@ from .abi import (BC_NEUMANN, BC_PERIODIC, CONV_NONE, CONV_WENO5, CONV_WENO5_CHA
                   NsParams, halo_shape, make_params)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libns_b200.so")
+# NS_B200_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = os.environ.get("NS_B200_LIB") or os.path.join(HERE, "lib", "libns_b200.so")
 
 __all__ = ["Solver", "NsError", "make_params", "halo_shape", "load_library", "abi"]
 

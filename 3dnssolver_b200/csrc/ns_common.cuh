@@ -87,11 +87,11 @@ NS_HOST_DEVICE int fold(int i, int n, int periodic) {
 // ---------------------------------------------------------------------------
 // WENO-5 (Jiang-Shu smoothness indicators, src/convection_schemes/weno-5.cpp:222-322)
 //
-// The three nonlinear weights are formed with a single division: with
+// The three nonlinear weights are formed without a division each: with
 // s_k = eps + beta_k (Shu) the weights d_k/s_k^2 normalised by their sum equal
-// d_k * prod_{j!=k} s_j^2 / sum_m d_m prod_{j!=m} s_j^2 (Borges: d_k (B_k+tau) prod_{j!=k} B_j).
-// The algebra is exact; results differ from the reference's three-division
-// form by rounding only.  Single precision keeps per-weight reciprocals
+// d_k * prod_{j!=k} s_j^2 / sum_m d_m prod_{j!=m} s_j^2 (Borges: d_k (B_k+tau) prod_{j!=k} B_j),
+// and the left and right reconstructions of one face share one division.
+// The algebra is exact; results differ from the reference's form by rounding only.  Single precision keeps per-weight reciprocals
 // (products of squares would leave the float range) and raises eps above the
 // float rounding floor of beta: eps32 = max(eps, (8 u32 s)^2), s the largest
 // |f| of the stencil.
@@ -120,14 +120,15 @@ __device__ __forceinline__ void weno_betas(T a, T b, T c, T d, T e, T& b0, T& b1
     b2 = k1312 * t1 * t1 + k14 * t2 * t2;
 }
 
-// Weighted combination of the three candidate values f0,f1,f2 with linear
-// weights (d0,d1,d2) given the stencil (a..e).
+// Weights of one reconstruction from the stencil (a..e) and linear weights
+// (d0,d1,d2): n_k proportional to the nonlinear weights, with the common
+// factor left in (exact algebra, see above).
 template <typename T, bool BORGES>
-__device__ __forceinline__ T weno_combine(T a, T b, T c, T d, T e, T f0, T f1, T f2, T d0, T d1, T d2) {
+__device__ __forceinline__ void weno_weights(T a, T b, T c, T d, T e, T d0, T d1, T d2, T& n0, T& n1,
+                                             T& n2) {
     T b0, b1, b2;
     weno_betas(a, b, c, d, e, b0, b1, b2);
     if constexpr (sizeof(T) == 8) {
-        T n0, n1, n2;
         if constexpr (BORGES) {
             T tau = fabs(b0 - b2);
             T B0 = b0 + WenoC<T>::eps_borges, B1 = b1 + WenoC<T>::eps_borges,
@@ -142,45 +143,62 @@ __device__ __forceinline__ T weno_combine(T a, T b, T c, T d, T e, T f0, T f1, T
             n1 = d1 * (A0 * A2);
             n2 = d2 * (A0 * A1);
         }
-        return (n0 * f0 + n1 * f1 + n2 * f2) / (n0 + n1 + n2);
     } else {
-        T a0, a1, a2;
         if constexpr (BORGES) {
             T tau = fabsf(b0 - b2);
-            a0 = d0 * (T(1) + tau * __frcp_rn(b0 + WenoC<T>::eps_borges));
-            a1 = d1 * (T(1) + tau * __frcp_rn(b1 + WenoC<T>::eps_borges));
-            a2 = d2 * (T(1) + tau * __frcp_rn(b2 + WenoC<T>::eps_borges));
+            n0 = d0 * (T(1) + tau * __frcp_rn(b0 + WenoC<T>::eps_borges));
+            n1 = d1 * (T(1) + tau * __frcp_rn(b1 + WenoC<T>::eps_borges));
+            n2 = d2 * (T(1) + tau * __frcp_rn(b2 + WenoC<T>::eps_borges));
         } else {
             T s = fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fabsf(d))), fabsf(e));
             T fl = T(8) * T(5.9604645e-8) * s;
             T eps = fmaxf(WenoC<T>::eps_shu, fl * fl);
             T s0 = eps + b0, s1 = eps + b1, s2 = eps + b2;
-            a0 = d0 * __frcp_rn(s0 * s0);
-            a1 = d1 * __frcp_rn(s1 * s1);
-            a2 = d2 * __frcp_rn(s2 * s2);
+            n0 = d0 * __frcp_rn(s0 * s0);
+            n1 = d1 * __frcp_rn(s1 * s1);
+            n2 = d2 * __frcp_rn(s2 * s2);
         }
-        return (a0 * f0 + a1 * f1 + a2 * f2) * __frcp_rn(a0 + a1 + a2);
     }
 }
 
-// WENO5_left (weno-5.cpp:305-322): value at i+1/2 from the left-biased stencil a..e = i-2..i+2
+// WENO5_left (weno-5.cpp:305-322) as num/den: value at i+1/2 from the
+// left-biased stencil a..e = i-2..i+2.  The ENO candidates are kept at 6x
+// their value and the 1/6 goes into den.
 template <typename T, bool BORGES>
-__device__ __forceinline__ T weno_left(T a, T b, T c, T d, T e) {
-    const T s6 = T(1) / T(6);
-    T f0 = (T(2) * a - T(7) * b + T(11) * c) * s6;
-    T f1 = (-b + T(5) * c + T(2) * d) * s6;
-    T f2 = (T(2) * c + T(5) * d - e) * s6;
-    return weno_combine<T, BORGES>(a, b, c, d, e, f0, f1, f2, T(0.1), T(0.6), T(0.3));
+__device__ __forceinline__ void weno_left_nd(T a, T b, T c, T d, T e, T& num, T& den) {
+    T f0 = T(2) * a - T(7) * b + T(11) * c;
+    T f1 = -b + T(5) * c + T(2) * d;
+    T f2 = T(2) * c + T(5) * d - e;
+    T n0, n1, n2;
+    weno_weights<T, BORGES>(a, b, c, d, e, T(0.1), T(0.6), T(0.3), n0, n1, n2);
+    num = n0 * f0 + n1 * f1 + n2 * f2;
+    den = T(6) * (n0 + n1 + n2);
 }
 
-// WENO5_right (weno-5.cpp:285-303): value at i+1/2 from the right-biased stencil a..e = i-1..i+3
+// WENO5_right (weno-5.cpp:285-303) as num/den: value at i+1/2 from the
+// right-biased stencil a..e = i-1..i+3.
 template <typename T, bool BORGES>
-__device__ __forceinline__ T weno_right(T a, T b, T c, T d, T e) {
-    const T s6 = T(1) / T(6);
-    T f0 = (-a + T(5) * b + T(2) * c) * s6;
-    T f1 = (T(2) * b + T(5) * c - d) * s6;
-    T f2 = (T(11) * c - T(7) * d + T(2) * e) * s6;
-    return weno_combine<T, BORGES>(a, b, c, d, e, f0, f1, f2, T(0.3), T(0.6), T(0.1));
+__device__ __forceinline__ void weno_right_nd(T a, T b, T c, T d, T e, T& num, T& den) {
+    T f0 = -a + T(5) * b + T(2) * c;
+    T f1 = T(2) * b + T(5) * c - d;
+    T f2 = T(11) * c - T(7) * d + T(2) * e;
+    T n0, n1, n2;
+    weno_weights<T, BORGES>(a, b, c, d, e, T(0.3), T(0.6), T(0.1), n0, n1, n2);
+    num = n0 * f0 + n1 * f1 + n2 * f2;
+    den = T(6) * (n0 + n1 + n2);
+}
+
+// f = WENO5_left(l) + WENO5_right(r) with one division in FP64:
+// nL/dL + nR/dR = (nL dR + nR dL)/(dL dR); FP32 uses two fast reciprocals.
+template <typename T, bool BORGES>
+__device__ __forceinline__ T weno_pair(T l0, T l1, T l2, T l3, T l4, T r0, T r1, T r2, T r3, T r4) {
+    T nL, dL, nR, dR;
+    weno_left_nd<T, BORGES>(l0, l1, l2, l3, l4, nL, dL);
+    weno_right_nd<T, BORGES>(r0, r1, r2, r3, r4, nR, dR);
+    if constexpr (sizeof(T) == 8)
+        return (nL * dR + nR * dL) / (dL * dR);
+    else
+        return nL * __frcp_rn(dL) + nR * __frcp_rn(dR);
 }
 
 }  // namespace nsb

@@ -251,8 +251,16 @@ struct Eig {
     T vel[3], qn, ql, qm, q2, c, c2, H, Kpc, K2pc, inv2c;
 };
 
+template <typename T>
+__device__ __forceinline__ T trsqrt(T x) {
+    if constexpr (sizeof(T) == 8) return rsqrt(x); else return rsqrtf(x);
+}
+
+// Reference semantics (c2 = gamma/(p rho), convection_flux.cpp:139): one
+// r = rsqrt(p rho) gives c = sqrt(gamma) r, 1/(2c) = p rho r / (2 sqrt(gamma))
+// and K/(2 c2) = (gamma-1) p rho / (2 gamma) without a division.
 template <int DIR, bool PHYS, typename T>
-__device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma) {
+__device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma, T inv_gm1) {
     Eig<T> e;
     T rho = wa[0], p = wa[1];
     e.vel[0] = wa[2]; e.vel[1] = wa[3]; e.vel[2] = wa[4];
@@ -260,14 +268,23 @@ __device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma) {
     e.ql = Frame<DIR>::l_sg * e.vel[Frame<DIR>::l_ax];
     e.qm = Frame<DIR>::m_sg * e.vel[Frame<DIR>::m_ax];
     e.q2 = e.vel[0] * e.vel[0] + e.vel[1] * e.vel[1] + e.vel[2] * e.vel[2];
-    // reference: c2 = gamma/(p rho) (convection_flux.cpp:139)
-    e.c2 = PHYS ? gamma * p * trcp(rho) : gamma * trcp(p * rho);
-    e.c = tsqrt(e.c2);
     T K = gamma - T(1);
-    e.H = e.c2 * trcp(K) + T(0.5) * e.q2;
-    e.Kpc = K * trcp(T(2) * e.c2);
+    if constexpr (PHYS) {
+        e.c2 = gamma * p * trcp(rho);
+        e.c = tsqrt(e.c2);
+        e.Kpc = K * T(0.5) * trcp(e.c2);
+        e.inv2c = T(0.5) * trcp(e.c);
+    } else {
+        T pr = p * rho;
+        T r = trsqrt(pr);
+        T sg = tsqrt(gamma);  // uniform across the warp; folded by the compiler per launch
+        e.c = sg * r;
+        e.c2 = gamma * (r * r);
+        e.Kpc = (K * T(0.5) / gamma) * pr;
+        e.inv2c = (T(0.5) / sg) * (pr * r);
+    }
+    e.H = e.c2 * inv_gm1 + T(0.5) * e.q2;
     e.K2pc = T(2) * e.Kpc;  // K/c2
-    e.inv2c = trcp(T(2) * e.c);
     return e;
 }
 
@@ -294,8 +311,30 @@ __device__ __forceinline__ T lproj(const Eig<T>& e, const T f[5]) {
     }
 }
 
+// Minimum resident blocks per SM requested from the register allocator for the
+// face kernels (128 threads each), per form.  Chosen by a sweep on B200 at
+// 256^3 (1, 3, 4 for FP64; 1, 5, 6 for FP32 characteristic): the caps trade a
+// few spilled registers for 12-20 resident warps instead of 8.
+#ifndef NS_FACE_MINB_F64CHAR
+#define NS_FACE_MINB_F64CHAR 3
+#endif
+#ifndef NS_FACE_MINB_F64COMP
+#define NS_FACE_MINB_F64COMP 4
+#endif
+#ifndef NS_FACE_MINB_F32CHAR
+#define NS_FACE_MINB_F32CHAR 5
+#endif
+#ifndef NS_FACE_MINB_F32COMP
+#define NS_FACE_MINB_F32COMP 1
+#endif
+template <bool CHAR, typename T>
+struct FaceMinBlocks {
+    static constexpr int value = sizeof(T) == 8 ? (CHAR ? NS_FACE_MINB_F64CHAR : NS_FACE_MINB_F64COMP)
+                                                : (CHAR ? NS_FACE_MINB_F32CHAR : NS_FACE_MINB_F32COMP);
+};
+
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
-__global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
+__global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value) k_face_flux(const double* __restrict__ W,
                                                    const double* __restrict__ U, Box b, Consts c,
                                                    TF* __restrict__ F, FaceBox fb) {
     int kk = blockIdx.x * 32 + threadIdx.x;
@@ -310,9 +349,11 @@ __global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
 
     T fL[5][5], fR[5][5];  // [variable][stencil]
     T wa[5];
-    T alpha = T(3);  // ConvectionFlux::max_eigenvalue returns 3.0 everywhere (convection_flux.cpp:241)
+    // ConvectionFlux::max_eigenvalue returns 3.0 everywhere (convection_flux.cpp:241)
+    T halpha = T(1.5);
     T Fc[6][5], Uc[6][5];
     (void)Fc; (void)Uc;
+    const T hg = half * gamma * inv_gm1;  // gamma/(2(gamma-1))
 #pragma unroll
     for (int s = 0; s < 6; s++) {
         long long o = o0 + s * step;
@@ -332,29 +373,30 @@ __global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
                 for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + w[q]);
             }
         }
-        // Euler flux along DIR (ConvectionFlux::form_flux, convection_flux.cpp:23-61)
+        // half the Euler flux along DIR (ConvectionFlux::form_flux, convection_flux.cpp:23-61);
+        // rho q_n H = q_n (gamma p/(gamma-1) + rho |u|^2/2) needs no division
         T rho = w[0], p = w[1];
         T qn = w[2 + DIR];
-        T c2 = gamma * p * trcp(rho);
-        T H = c2 * inv_gm1 + half * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-        T rq = rho * qn;
+        T hrq = half * rho * qn;
+        T ke = w[2] * w[2] + w[3] * w[3] + w[4] * w[4];
         T f[5];
-        f[0] = rq;
-        f[1] = rq * H;
-        f[2] = rq * w[2] + (DIR == 0 ? p : T(0));
-        f[3] = rq * w[3] + (DIR == 1 ? p : T(0));
-        f[4] = rq * w[4] + (DIR == 2 ? p : T(0));
+        f[0] = hrq;
+        f[1] = qn * (hg * p + T(0.25) * rho * ke);
+        f[2] = hrq * w[2] + (DIR == 0 ? half * p : T(0));
+        f[3] = hrq * w[3] + (DIR == 1 ? half * p : T(0));
+        f[4] = hrq * w[4] + (DIR == 2 ? half * p : T(0));
         if constexpr (PHYS) {
             // local Lax-Friedrichs speed max(|qn|+c) over the 6-cell stencil
-            T a = fabs(qn) + tsqrt(c2);
-            alpha = (s == 0) ? a : (a > alpha ? a : alpha);
+            T a = half * (fabs(qn) + tsqrt(gamma * p * trcp(rho)));
+            halpha = (s == 0) ? a : (a > halpha ? a : halpha);
 #pragma unroll
             for (int q = 0; q < 5; q++) { Fc[s][q] = f[q]; Uc[s][q] = u[q]; }
         } else {
+            // fL = (F + alpha U)/2, fR = (F - alpha U)/2
 #pragma unroll
             for (int q = 0; q < 5; q++) {
-                if (s <= 4) fL[q][s] = (f[q] + alpha * u[q]) * half;
-                if (s >= 1) fR[q][s - 1] = (f[q] - alpha * u[q]) * half;
+                if (s <= 4) fL[q][s] = halpha * u[q] + f[q];
+                if (s >= 1) fR[q][s - 1] = f[q] - halpha * u[q];
             }
         }
     }
@@ -363,8 +405,8 @@ __global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
         for (int s = 0; s < 6; s++)
 #pragma unroll
             for (int q = 0; q < 5; q++) {
-                if (s <= 4) fL[q][s] = (Fc[s][q] + alpha * Uc[s][q]) * half;
-                if (s >= 1) fR[q][s - 1] = (Fc[s][q] - alpha * Uc[s][q]) * half;
+                if (s <= 4) fL[q][s] = halpha * Uc[s][q] + Fc[s][q];
+                if (s >= 1) fR[q][s - 1] = Fc[s][q] - halpha * Uc[s][q];
             }
     }
 
@@ -372,10 +414,10 @@ __global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
     if constexpr (!CHAR) {
 #pragma unroll
         for (int q = 0; q < 5; q++)
-            out[q] = weno_left<T, BORGES>(fL[q][0], fL[q][1], fL[q][2], fL[q][3], fL[q][4]) +
-                     weno_right<T, BORGES>(fR[q][0], fR[q][1], fR[q][2], fR[q][3], fR[q][4]);
+            out[q] = weno_pair<T, BORGES>(fL[q][0], fL[q][1], fL[q][2], fL[q][3], fL[q][4],
+                                          fR[q][0], fR[q][1], fR[q][2], fR[q][3], fR[q][4]);
     } else {
-        Eig<T> e = make_eig<DIR, PHYS, T>(wa, gamma);
+        Eig<T> e = make_eig<DIR, PHYS, T>(wa, gamma, inv_gm1);
         T ft[5];
         // characteristic projection L fL, L fR per stencil column, WENO per field
         // (Weno5cw::compute_num_flux, weno-5cw.cpp:4-28)
@@ -388,8 +430,8 @@ __global__ void __launch_bounds__(128) k_face_flux(const double* __restrict__ W,
                 cl[s] = lproj<DIR, PHYS, RR, T>(e, vl);                          \
                 cr[s] = lproj<DIR, PHYS, RR, T>(e, vr);                          \
             }                                                                    \
-            ft[RR] = weno_left<T, BORGES>(cl[0], cl[1], cl[2], cl[3], cl[4]) +   \
-                     weno_right<T, BORGES>(cr[0], cr[1], cr[2], cr[3], cr[4]);   \
+            ft[RR] = weno_pair<T, BORGES>(cl[0], cl[1], cl[2], cl[3], cl[4],      \
+                                          cr[0], cr[1], cr[2], cr[3], cr[4]);     \
         }
         NS_CHAR_FIELD(0)
         NS_CHAR_FIELD(1)
