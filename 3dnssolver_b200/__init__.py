@@ -47,6 +47,7 @@ def load_library():
     P = ctypes.POINTER(NsParams)
     C = ctypes.c_void_p
     dp = ctypes.POINTER(ctypes.c_double)
+    fp = ctypes.POINTER(ctypes.c_float)
     st = ctypes.c_int
     protos = {
         "ns_status_string": ([st], ctypes.c_char_p),
@@ -70,6 +71,14 @@ def load_library():
         "ns_get_diagnostics": ([C, ctypes.POINTER(NsDiagnostics)], st),
         "ns_kernel_launches": ([C], ctypes.c_longlong),
         "ns_profile_step": ([C, ctypes.POINTER(ctypes.c_float), ctypes.c_int], st),
+        "ns_sensor_init": ([ctypes.c_ulonglong, fp], st),
+        "ns_sensor_harvest": ([C, C, C, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong),
+                               ctypes.c_double], st),
+        "ns_sensor_train": ([C, C, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                             ctypes.c_float, ctypes.c_ulonglong, fp, fp, C], st),
+        "ns_sensor_gradients": ([C, C, ctypes.c_int, ctypes.c_float, fp, fp, fp, C], st),
+        "ns_sensor_predict": ([C, ctypes.c_longlong, fp, C, C], st),
+        "ns_set_sensor_weights": ([C, fp], st),
     }
     for name, (args, res) in protos.items():
         f = getattr(L, name)
@@ -87,6 +96,55 @@ def _check(status, what):
 
 def _dptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _fptr(a):
+    assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+# ---------------------------------------------------------------------------
+# learned face sensor (device buffers are passed as integer device pointers,
+# e.g. torch.Tensor.data_ptr())
+
+SENSOR_FEATURES = 21
+SENSOR_NPARAMS = 2145
+
+
+def sensor_init(seed):
+    w = np.zeros(SENSOR_NPARAMS, dtype=np.float32)
+    _check(load_library().ns_sensor_init(int(seed), _fptr(w)), "ns_sensor_init")
+    return w
+
+
+def sensor_train(feat_ptr, label_ptr, n, w, *, epochs=5, batch=65536, lr=1e-3, pos_weight=1.0,
+                 seed=0, stream=0):
+    """Adam training on device samples; returns (new weights, per-epoch mean loss)."""
+    w = np.ascontiguousarray(w, dtype=np.float32).copy()
+    losses = np.zeros(epochs, dtype=np.float32)
+    _check(load_library().ns_sensor_train(ctypes.c_void_p(feat_ptr), ctypes.c_void_p(label_ptr),
+                                          int(n), int(epochs), int(batch), float(lr),
+                                          float(pos_weight), int(seed), _fptr(w), _fptr(losses),
+                                          ctypes.c_void_p(stream)), "ns_sensor_train")
+    return w, losses
+
+
+def sensor_gradients(feat_ptr, label_ptr, n, w, pos_weight=1.0, stream=0):
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    g = np.zeros(SENSOR_NPARAMS, dtype=np.float32)
+    loss = np.zeros(1, dtype=np.float32)
+    _check(load_library().ns_sensor_gradients(ctypes.c_void_p(feat_ptr), ctypes.c_void_p(label_ptr),
+                                              int(n), float(pos_weight), _fptr(w), _fptr(g),
+                                              _fptr(loss), ctypes.c_void_p(stream)),
+           "ns_sensor_gradients")
+    return g, float(loss[0])
+
+
+def sensor_predict(feat_ptr, n, w, logit_ptr, stream=0):
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    _check(load_library().ns_sensor_predict(ctypes.c_void_p(feat_ptr), int(n), _fptr(w),
+                                            ctypes.c_void_p(logit_ptr), ctypes.c_void_p(stream)),
+           "ns_sensor_predict")
 
 
 class Solver:
@@ -202,6 +260,24 @@ class Solver:
             "enstrophy": d.enstrophy, "nonfinite": bool(d.nonfinite),
             "sensor_fraction": d.sensor_fraction,
         }
+
+    def sensor_harvest(self, feat_ptr, label_ptr, capacity, rel_threshold=1e-3):
+        """Features/labels of every face of the current state into device buffers; returns the row count."""
+        cnt = ctypes.c_longlong()
+        _check(self.lib.ns_sensor_harvest(self.h, ctypes.c_void_p(feat_ptr), ctypes.c_void_p(label_ptr),
+                                          int(capacity), ctypes.byref(cnt), float(rel_threshold)),
+               "ns_sensor_harvest")
+        return cnt.value
+
+    def set_sensor_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(self.lib.ns_set_sensor_weights(self.h, _fptr(w)), "ns_set_sensor_weights")
+
+    def faces(self):
+        """Faces per stage along the convected axes (rows of one harvest)."""
+        p = self.params
+        n = [(p.nx + 1) * p.ny * p.nz, p.nx * (p.ny + 1) * p.nz, p.nx * p.ny * (p.nz + 1)]
+        return sum(n[:3 if p.dim == 3 else 2])
 
     PROFILE_CLASSES = ("step_begin", "fill_prim", "face_x", "face_y", "face_z", "update")
 

@@ -219,8 +219,11 @@ static ns_status faces(ns_ctx* ctx) {
     int nd = p.dim == 3 ? 3 : 2;
     for (int d = 0; d < nd; d++) {
         if (p.sensor) {
-            NS_TRY(sensor_face_flux(ctx->sensor, d, ctx->W, ctx->U, ctx->box, ctx->c, ctx->F[d],
-                                    ctx->fb[d], ctx->stream, &ctx->launches));
+            if (sensor_face_flux(ctx->sensor, d, ctx->W, ctx->U, ctx->box, ctx->c, p.sensor_threshold,
+                                 p.weights == NS_WEIGHTS_BORGES, ctx->F[d], ctx->fb[d], ctx->stream,
+                                 &ctx->launches) != NS_OK)
+                return fail(NS_ERR_CUDA, "gated face kernel launch failed: %s",
+                            cudaGetErrorString(cudaGetLastError()));
         } else {
             launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
                              phys(ctx), fp32(ctx), ctx->W, ctx->U, ctx->box, ctx->c, ctx->F[d],
@@ -621,6 +624,45 @@ ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
 }
 
 long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+ns_status ns_set_sensor_weights(ns_ctx* ctx, const float* w) {
+    if (!ctx || !w) return fail(NS_ERR_INVALID_ARG, "ctx and w must be non-NULL");
+    if (!ctx->sensor) return fail(NS_ERR_INVALID_ARG, "the context was created without the sensor (params.sensor = 0)");
+    if (sensor_set_weights(ctx->sensor, w, ctx->stream) != NS_OK)
+        return fail(NS_ERR_CUDA, "uploading the sensor weights failed");
+    return NS_OK;
+}
+
+ns_status ns_sensor_harvest(ns_ctx* ctx, float* feat, float* label, long long capacity, long long* count,
+                            double rel_threshold) {
+    if (!ctx || !feat || !label || !count) return fail(NS_ERR_INVALID_ARG, "NULL argument");
+    if (!ctx->w_valid && !ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no state has been uploaded");
+    if (!(rel_threshold > 0.0)) return fail(NS_ERR_INVALID_ARG, "rel_threshold must be > 0");
+    const int nd = ctx->p.dim == 3 ? 3 : 2;
+    long long need = 0;
+    for (int d = 0; d < nd; d++) need += (long long)ctx->fb[d].n0 * ctx->fb[d].n1 * ctx->fb[d].n2;
+    *count = need;
+    if (need > capacity)
+        return fail(NS_ERR_INVALID_ARG, "harvest needs %lld rows, capacity is %lld", need, capacity);
+    cudaStream_t s = ctx->stream;
+    // the stage-1 view of the current state: U = cons(W) on all cells, boundary fill, W = prim(U)
+    NS_TRY(finalize_w(ctx));
+    launch_cons_all(ctx->W, ctx->U, ctx->box, ctx->c, s);
+    launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
+    NS_TRY(check_launch(ctx, 2));
+    ctx->u_valid = true;
+    ctx->w_valid = true;
+    long long base = 0;
+    for (int d = 0; d < nd; d++) {
+        if (sensor_harvest(d, ctx->p.weights == NS_WEIGHTS_BORGES, ctx->W, ctx->U, ctx->box, ctx->c,
+                           ctx->fb[d], base, rel_threshold, feat, label, s) != NS_OK)
+            return fail(NS_ERR_CUDA, "harvest kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        NS_TRY(check_launch(ctx, 1));
+        base += (long long)ctx->fb[d].n0 * ctx->fb[d].n1 * ctx->fb[d].n2;
+    }
+    NS_CUDA(cudaStreamSynchronize(s));
+    return NS_OK;
+}
 
 }  // extern "C"
 

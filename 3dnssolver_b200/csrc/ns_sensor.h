@@ -15,8 +15,14 @@ void sensor_destroy(SensorState* st);
 // Gated face fluxes along axis dir: component-wise FP32 WENO on every face, the
 // characteristic-wise flux recomputed on the faces the sensor flags.
 ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const double* U, const Box& b,
-                           const Consts& c, void* F, const FaceBox& fb, cudaStream_t s,
-                           long long* launches);
+                           const Consts& c, double threshold, bool borges, void* F,
+                           const FaceBox& fb, cudaStream_t s, long long* launches);
+// fraction of evaluated faces the sensor flagged since the context was created
 double sensor_last_fraction(SensorState* st);
+ns_status sensor_set_weights(SensorState* st, const float* w, cudaStream_t s);
+// features + labels of the faces along dir into feat/label starting at row base
+ns_status sensor_harvest(int dir, bool borges, const double* W, const double* U, const Box& b,
+                         const Consts& c, const FaceBox& fb, long long base, double thr, float* feat,
+                         float* label, cudaStream_t s);
 
 }  // namespace nsb

@@ -164,6 +164,46 @@ enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FAC
  * between its kernels on the context's stream; ms[c] receives the device time
  * of kernel class c summed over the step (n >= NS_PROF_N). */
 NS_API ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n);
+/* ---- learned troubled-face sensor (no reference counterpart) ----------------
+ * An MLP 21 -> 32 -> 32 -> 1 (GELU) predicts from a face's stencil whether the
+ * characteristic-wise WENO-5 flux differs from the component-wise one by more
+ * than a relative threshold; with ns_params.sensor = 1 (FP32 characteristic
+ * form) the component-wise flux is used on every face and the characteristic
+ * one is recomputed on the faces the network flags.  Parameters are
+ * NS_SENSOR_NPARAMS floats: W1[32][32] (out, in; in >= 21 unused), b1[32],
+ * W2[32][32], b2[32], w3[32], b3.  Device pointers below are caller-owned. */
+#define NS_SENSOR_FEATURES 21
+#define NS_SENSOR_NPARAMS 2145
+/* Glorot-uniform weights and zero biases from a seed (host array). */
+NS_API ns_status ns_sensor_init(unsigned long long seed, float* w);
+/* Features (NS_SENSOR_FEATURES floats per face) and labels (0/1) of every face
+ * of the context's current state along each convected axis, from FP64
+ * component- and characteristic-wise fluxes; label = |f_char - f_comp|_2 >
+ * rel_threshold (|f_char|_2 + 1e-12).  Appends nothing: rows 0..count-1 of the
+ * device arrays are written; capacity is their row count.  The context's
+ * state goes through one equation-of-state round trip (rounding level). */
+NS_API ns_status ns_sensor_harvest(ns_ctx* ctx, float* d_features, float* d_labels,
+                                   long long capacity, long long* count, double rel_threshold);
+/* Adam (lr, beta 0.9/0.999) on the binary cross-entropy with logits, positive
+ * class weighted by pos_weight, `epochs` passes over n samples in mini-batches
+ * of `batch` (a seeded permutation per epoch).  w (host) is updated in place;
+ * epoch_loss (host, may be NULL) receives the mean loss of each epoch.  BF16
+ * tensor-core forward and backward with FP32 accumulation. */
+NS_API ns_status ns_sensor_train(const float* d_features, const float* d_labels, long long n,
+                                 int epochs, int batch, float lr, float pos_weight,
+                                 unsigned long long seed, float* w, float* epoch_loss,
+                                 void* cuda_stream);
+/* Gradient (host, NS_SENSOR_NPARAMS) and mean loss of one batch of n samples. */
+NS_API ns_status ns_sensor_gradients(const float* d_features, const float* d_labels, int n,
+                                     float pos_weight, const float* w, float* grad, float* loss,
+                                     void* cuda_stream);
+/* Logits of n samples into d_logits. */
+NS_API ns_status ns_sensor_predict(const float* d_features, long long n, const float* w,
+                                   float* d_logits, void* cuda_stream);
+/* Installs the network a sensor-gated context uses (host array; until called
+ * the network is all zeros and never fires). */
+NS_API ns_status ns_set_sensor_weights(ns_ctx* ctx, const float* w);
+
 /* ---- convection residual without device allocation -------------------------
  * No counterpart in the reference.  For callers that may not allocate device
  * memory or have it allocated for them: hosts that serve all device memory
