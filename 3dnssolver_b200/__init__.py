@@ -279,12 +279,14 @@ class Solver:
         n = [(p.nx + 1) * p.ny * p.nz, p.nx * (p.ny + 1) * p.nz, p.nx * p.ny * (p.nz + 1)]
         return sum(n[:3 if p.dim == 3 else 2])
 
-    PROFILE_CLASSES = ("step_begin", "fill_prim", "face_x", "face_y", "face_z", "update")
+    PROFILE_CLASSES = ("step_begin", "fill_prim", "face_x", "face_y", "face_z", "update",
+                       "stage_fused")
 
     def profile_step(self):
         """One device-resident step with events between kernels: {kernel class: ms}."""
-        ms = (ctypes.c_float * 6)()
-        _check(self.lib.ns_profile_step(self.h, ms, 6), "ns_profile_step")
+        n = len(self.PROFILE_CLASSES)
+        ms = (ctypes.c_float * n)()
+        _check(self.lib.ns_profile_step(self.h, ms, n), "ns_profile_step")
         return dict(zip(self.PROFILE_CLASSES, [float(x) for x in ms]))
 
     @property

@@ -146,17 +146,17 @@ __device__ __forceinline__ void weno_weights(T a, T b, T c, T d, T e, T d0, T d1
     } else {
         if constexpr (BORGES) {
             T tau = fabsf(b0 - b2);
-            n0 = d0 * (T(1) + tau * __frcp_rn(b0 + WenoC<T>::eps_borges));
-            n1 = d1 * (T(1) + tau * __frcp_rn(b1 + WenoC<T>::eps_borges));
-            n2 = d2 * (T(1) + tau * __frcp_rn(b2 + WenoC<T>::eps_borges));
+            n0 = d0 * (T(1) + __fdividef(tau, b0 + WenoC<T>::eps_borges));
+            n1 = d1 * (T(1) + __fdividef(tau, b1 + WenoC<T>::eps_borges));
+            n2 = d2 * (T(1) + __fdividef(tau, b2 + WenoC<T>::eps_borges));
         } else {
             T s = fmaxf(fmaxf(fmaxf(fabsf(a), fabsf(b)), fmaxf(fabsf(c), fabsf(d))), fabsf(e));
             T fl = T(8) * T(5.9604645e-8) * s;
             T eps = fmaxf(WenoC<T>::eps_shu, fl * fl);
             T s0 = eps + b0, s1 = eps + b1, s2 = eps + b2;
-            n0 = d0 * __frcp_rn(s0 * s0);
-            n1 = d1 * __frcp_rn(s1 * s1);
-            n2 = d2 * __frcp_rn(s2 * s2);
+            n0 = __fdividef(d0, s0 * s0);
+            n1 = __fdividef(d1, s1 * s1);
+            n2 = __fdividef(d2, s2 * s2);
         }
     }
 }
@@ -198,7 +198,7 @@ __device__ __forceinline__ T weno_pair(T l0, T l1, T l2, T l3, T l4, T r0, T r1,
     if constexpr (sizeof(T) == 8)
         return (nL * dR + nR * dL) / (dL * dR);
     else
-        return nL * __frcp_rn(dL) + nR * __frcp_rn(dR);
+        return __fdividef(nL, dL) + __fdividef(nR, dR);
 }
 
 }  // namespace nsb

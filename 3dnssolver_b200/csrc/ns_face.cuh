@@ -45,7 +45,7 @@ __device__ __forceinline__ T tsqrt(T x) {
 }
 template <typename T>
 __device__ __forceinline__ T trcp(T x) {
-    if constexpr (sizeof(T) == 8) return 1.0 / x; else return __frcp_rn(x);
+    if constexpr (sizeof(T) == 8) return 1.0 / x; else return __fdividef(1.0f, x);
 }
 
 // Left/right eigenvectors of the 3D Euler Jacobian (ConvectionFlux::eigenvectors,
@@ -125,6 +125,49 @@ __device__ __forceinline__ long long face_origin(const Box& b, int aa, int bb, i
     return b.at(ih, jh, kh);
 }
 
+// Half the Euler flux of one cell along DIR (ConvectionFlux::form_flux,
+// convection_flux.cpp:23-61): rho q_n H = q_n (gamma p/(gamma-1) + rho |u|^2/2)
+// needs no division.  hg = gamma/(2(gamma-1)).
+template <int DIR, typename T>
+__device__ __forceinline__ void half_flux(const T w[5], T hg, T f[5]) {
+    const T half = T(0.5);
+    T rho = w[0], p = w[1];
+    T qn = w[2 + DIR];
+    T hrq = half * rho * qn;
+    T ke = w[2] * w[2] + w[3] * w[3] + w[4] * w[4];
+    f[0] = hrq;
+    f[1] = qn * (hg * p + T(0.25) * rho * ke);
+    f[2] = hrq * w[2] + (DIR == 0 ? half * p : T(0));
+    f[3] = hrq * w[3] + (DIR == 1 ? half * p : T(0));
+    f[4] = hrq * w[4] + (DIR == 2 ? half * p : T(0));
+}
+
+// Lax-Friedrichs split of stencil cell s (reference semantics: alpha = 3):
+// fL = (F + alpha U)/2 for s = 0..4, fR = (F - alpha U)/2 for s = 1..5; the
+// face average of W is taken from cells 2 and 3.
+template <int DIR, bool CHAR, typename T>
+__device__ __forceinline__ void split_cell(int s, const T w[5], const T u[5], T hg, T fL[5][5],
+                                           T fR[5][5], T wa[5]) {
+    const T halpha = T(1.5), half = T(0.5);
+    if constexpr (CHAR) {
+        if (s == 2) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) wa[q] = w[q];
+        }
+        if (s == 3) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + w[q]);
+        }
+    }
+    T f[5];
+    half_flux<DIR, T>(w, hg, f);
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        if (s <= 4) fL[q][s] = halpha * u[q] + f[q];
+        if (s >= 1) fR[q][s - 1] = f[q] - halpha * u[q];
+    }
+}
+
 // stencil load + Euler flux + Lax-Friedrichs split; wa receives the face
 // average of W (characteristic form only)
 template <int DIR, bool CHAR, bool PHYS, typename T>
@@ -132,58 +175,46 @@ __device__ __forceinline__ void face_stencil(const double* __restrict__ W, const
                                              const Box& b, const Consts& c, long long o0,
                                              long long step, T fL[5][5], T fR[5][5], T wa[5]) {
     const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1), half = T(0.5);
-    // ConvectionFlux::max_eigenvalue returns 3.0 everywhere (convection_flux.cpp:241)
-    T halpha = T(1.5);
-    T Fc[6][5], Uc[6][5];
-    (void)Fc; (void)Uc;
     const T hg = half * gamma * inv_gm1;  // gamma/(2(gamma-1))
+    if constexpr (!PHYS) {
 #pragma unroll
-    for (int s = 0; s < 6; s++) {
-        long long o = o0 + s * step;
-        T w[5], u[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            w[q] = T(W[q * b.fstride + o]);
-            u[q] = T(U[q * b.fstride + o]);
-        }
-        if constexpr (CHAR) {
-            if (s == 2) {
-#pragma unroll
-                for (int q = 0; q < 5; q++) wa[q] = w[q];
-            }
-            if (s == 3) {
-#pragma unroll
-                for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + w[q]);
-            }
-        }
-        // half the Euler flux along DIR (ConvectionFlux::form_flux, convection_flux.cpp:23-61);
-        // rho q_n H = q_n (gamma p/(gamma-1) + rho |u|^2/2) needs no division
-        T rho = w[0], p = w[1];
-        T qn = w[2 + DIR];
-        T hrq = half * rho * qn;
-        T ke = w[2] * w[2] + w[3] * w[3] + w[4] * w[4];
-        T f[5];
-        f[0] = hrq;
-        f[1] = qn * (hg * p + T(0.25) * rho * ke);
-        f[2] = hrq * w[2] + (DIR == 0 ? half * p : T(0));
-        f[3] = hrq * w[3] + (DIR == 1 ? half * p : T(0));
-        f[4] = hrq * w[4] + (DIR == 2 ? half * p : T(0));
-        if constexpr (PHYS) {
-            // local Lax-Friedrichs speed max(|qn|+c) over the 6-cell stencil
-            T a = half * (fabs(qn) + tsqrt(gamma * p * trcp(rho)));
-            halpha = (s == 0) ? a : (a > halpha ? a : halpha);
-#pragma unroll
-            for (int q = 0; q < 5; q++) { Fc[s][q] = f[q]; Uc[s][q] = u[q]; }
-        } else {
-            // fL = (F + alpha U)/2, fR = (F - alpha U)/2
+        for (int s = 0; s < 6; s++) {
+            long long o = o0 + s * step;
+            T w[5], u[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) {
-                if (s <= 4) fL[q][s] = halpha * u[q] + f[q];
-                if (s >= 1) fR[q][s - 1] = f[q] - halpha * u[q];
+                w[q] = T(W[q * b.fstride + o]);
+                u[q] = T(U[q * b.fstride + o]);
             }
+            split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
         }
-    }
-    if constexpr (PHYS) {
+    } else {
+        // local Lax-Friedrichs speed max(|qn|+c) over the 6-cell stencil: the split
+        // waits until every cell's speed is known
+        T Fc[6][5], Uc[6][5], halpha = T(0);
+#pragma unroll
+        for (int s = 0; s < 6; s++) {
+            long long o = o0 + s * step;
+            T w[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                w[q] = T(W[q * b.fstride + o]);
+                Uc[s][q] = T(U[q * b.fstride + o]);
+            }
+            if constexpr (CHAR) {
+                if (s == 2) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) wa[q] = w[q];
+                }
+                if (s == 3) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + w[q]);
+                }
+            }
+            half_flux<DIR, T>(w, hg, Fc[s]);
+            T a = half * (fabs(w[2 + DIR]) + tsqrt(gamma * w[1] * trcp(w[0])));
+            halpha = (s == 0) ? a : (a > halpha ? a : halpha);
+        }
 #pragma unroll
         for (int s = 0; s < 6; s++)
 #pragma unroll
@@ -192,7 +223,6 @@ __device__ __forceinline__ void face_stencil(const double* __restrict__ W, const
                 if (s >= 1) fR[q][s - 1] = Fc[s][q] - halpha * Uc[s][q];
             }
     }
-
 }
 
 // component-wise: f_q = WENO5_left(fL_q) + WENO5_right(fR_q)   (weno-5.cpp:96-114)

@@ -15,67 +15,12 @@
 #include <cmath>
 
 #include "ns_common.cuh"
+#include "ns_eos.cuh"
 #include "ns_face.cuh"
 #include "ns_kernels.h"
+#include "ns_viscous.cuh"
 
 namespace nsb {
-
-// ---------------------------------------------------------------------------
-// equation of state (src/eq_of_state.cpp:32-87)
-
-__device__ __forceinline__ void prim_from_cons(const double u[5], double gm1, double w[5]) {
-    double ir = 1.0 / u[0];
-    w[0] = u[0];
-    w[2] = u[2] * ir;
-    w[3] = u[3] * ir;
-    w[4] = u[4] * ir;
-    double kin = 0.5 * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-    w[1] = gm1 * (u[1] - u[0] * kin);
-}
-
-__device__ __forceinline__ void cons_from_prim(const double w[5], double inv_gm1, double u[5]) {
-    u[0] = w[0];
-    u[2] = w[0] * w[2];
-    u[3] = w[0] * w[3];
-    u[4] = w[0] * w[4];
-    double kin = 0.5 * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-    u[1] = w[1] * inv_gm1 + kin;
-}
-
-// EqOfState::local_dt (src/eq_of_state.cpp:89-101), min over directions
-__device__ __forceinline__ double local_dt(const double w[5], const Consts& c) {
-    double cs = sqrt(c.gamma * w[1] / w[0]);
-    double ex = c.dx / fmax(fabs(w[2] + cs), fabs(w[2] - cs));
-    double ey = c.dy / fmax(fabs(w[3] + cs), fabs(w[3] - cs));
-    double ez = c.dz / fmax(fabs(w[4] + cs), fabs(w[4] - cs));
-    double t = (ey < ex) ? ey : ex;
-    return (ez < t) ? ez : t;
-}
-
-__device__ __forceinline__ double local_dt_physical(const double w[5], const Consts& c) {
-    double cs = sqrt(c.gamma * w[1] / w[0]);
-    double r = (fabs(w[2]) + cs) * c.inv_dx + (fabs(w[3]) + cs) * c.inv_dy;
-    if (c.dim == 3) r += (fabs(w[4]) + cs) * c.inv_dz;
-    return 1.0 / r;
-}
-
-// block-wide min of a positive double, then one 64-bit atomicMin on its bit
-// pattern (positive IEEE doubles order like their unsigned bit patterns)
-__device__ __forceinline__ void block_min_to(double v, unsigned long long* slot) {
-    __shared__ double red[32];
-    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-    int lane = (threadIdx.x + threadIdx.y * blockDim.x) & 31;
-    int warp = (threadIdx.x + threadIdx.y * blockDim.x) >> 5;
-    int nw = (blockDim.x * blockDim.y + 31) >> 5;
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        v = lane < nw ? red[lane] : INFINITY;
-        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-        if (lane == 0 && v < INFINITY)
-            atomicMin(slot, (unsigned long long)__double_as_longlong(v));
-    }
-}
 
 // ---------------------------------------------------------------------------
 // step begin: dt from W at the step start (TimeScheme::set_dt), then
@@ -328,34 +273,8 @@ __device__ __forceinline__ void viscous_reference(const double* __restrict__ W, 
         }
         Dxy[v] = sxy; Dyx[v] = syx;
     }
-    const TV mu = TV(c.mu), lamb = TV(c.lamb), two = TV(2);
-    const TV Uc = TV(W[2 * fs + o]), Vc = TV(W[3 * fs + o]), P = TV(W[1 * fs + o]),
-             RHO = TV(W[o]);
-    const TV du_dx = Dx[2], du_dy = Dy[2], du_dxdx = Dxx[2], du_dydy = Dyy[2];
-    const TV du_dxdy = Dxy[0], du_dydx = Dyx[0];
-    const TV dv_dy = Dy[3], dv_dx = Dx[3], dv_dxdx = Dxx[3], dv_dydy = Dyy[3];
-    const TV dv_dydx = Dyx[1], dv_dxdy = Dxy[1];
-    const TV drho_dx = Dx[0], dp_dx = Dx[1], drho_dxdx = Dxx[0], dp_dxdx = Dxx[1];
-    const TV drho_dy = Dy[0], dp_dy = Dy[1], drho_dydy = Dyy[0], dp_dydy = Dyy[1];
-
-    TV Dtauxx_dx = two * mu * du_dxdx + lamb * (du_dxdx + dv_dydx);
-    TV Dtauyy_dy = two * mu * dv_dydy + lamb * (du_dxdy + dv_dydy);
-    TV Dtauxy_dx = mu * (du_dydx + dv_dxdx);
-    TV Dtauyx_dy = mu * (du_dydy + dv_dxdy);
-    TV Tauxx = two * mu * du_dx + lamb * (du_dx + dv_dy);
-    TV Tauyy = Tauxx;
-    TV Tauxy = mu * (du_dy + dv_dx);
-    TV Dtauvx_dx = Uc * Dtauxx_dx + Vc * Dtauxy_dx + Tauxx * du_dx + Tauxy * dv_dy;
-    TV Dtauvy_dy = Uc * Dtauyx_dy + Vc * Dtauyy_dy + Tauyy * dv_dy + Tauxy * du_dy;
-    TV ir = TV(1) / RHO, ir2 = ir * ir, ir3 = ir2 * ir;
-    TV heat = TV(c.heat);
-    TV Dqx_dx = -heat * (mu * (two * ir2 * drho_dx * dp_dx + ir * dp_dxdx + ir3 * P * drho_dx * drho_dx -
-                               ir2 * P * drho_dxdx));
-    TV Dqy_dy = -heat * (mu * (two * ir2 * drho_dy * dp_dy + ir * dp_dydy + ir3 * drho_dy * drho_dy -
-                               ir2 * P * drho_dydy));
-    r[1] += -Dtauvx_dx - Dtauvy_dy + Dqx_dx + Dqy_dy;
-    r[2] += -Dtauxx_dx - Dtauyx_dy;
-    r[3] += -Dtauyy_dy - Dtauxy_dx;
+    viscous_reference_terms<TV>(Dx, Dy, Dxx, Dyy, Dxy, Dyx, TV(W[2 * fs + o]), TV(W[3 * fs + o]),
+                                TV(W[1 * fs + o]), TV(W[o]), c, r);
 }
 
 // Physical semantics: full 3D viscous stress and heat flux with constant mu
@@ -439,8 +358,13 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
 //   MODE_RHS  : Rout += R
 // dt = CFL * min(1e10, reduced minimum) (time_scheme.cpp:98-136).
 
+// The update kernel is memory-latency bound; 8 resident blocks (64 registers)
+// matched the compiler's own choice and beat looser bounds in a B200 sweep.
+#ifndef NS_UPDATE_MINB
+#define NS_UPDATE_MINB 8
+#endif
 template <int MODE, int H, bool PHYS, typename TF, typename TV>
-__global__ void __launch_bounds__(128) k_update(const double* __restrict__ W, double* __restrict__ U,
+__global__ void __launch_bounds__(128, NS_UPDATE_MINB) k_update(const double* __restrict__ W, double* __restrict__ U,
                                                 const double* __restrict__ U0,
                                                 const TF* __restrict__ Fx, const TF* __restrict__ Fy,
                                                 const TF* __restrict__ Fz, Box b, FaceBox fx,

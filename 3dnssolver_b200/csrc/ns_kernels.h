@@ -29,6 +29,23 @@ struct UpdateArgs {
     double* clock;                   // [last dt, accumulated time], updated once per step (nullable)
 };
 
+// one fused SSP-RK3 stage (ns_fused.cu)
+struct FusedArgs {
+    const double* Uin;
+    double* U0;
+    double* Uout;
+    Box b;
+    Consts c;
+    int conv_dims;   // 0 (no convection), 2 or 3
+    int visc_h;      // half width of the CD stencil, 0 without diffusion
+    bool fp32, chr, borges, last;
+    double m1, m2, mc;
+    const unsigned long long* slot;   // CFL minimum of this step
+    unsigned long long* slot_next;    // last stage: CFL minimum of the next step
+    double* clock;                    // first stage: [last dt, accumulated time]
+};
+cudaError_t launch_stage_fused(const FusedArgs& a, cudaStream_t s);
+
 void launch_step_begin(bool from_u, bool phys, double* W, double* U, double* U0, const Box& b,
                        const Consts& c, unsigned long long* slot, cudaStream_t s);
 void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s);

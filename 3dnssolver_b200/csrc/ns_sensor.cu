@@ -1,6 +1,6 @@
 // ns_sensor.cu -- learned troubled-face sensor (no reference counterpart).
 //
-// A small MLP (21 -> 32 -> 32 -> 1, GELU) looks at the stencil of a face and
+// A small MLP (21 -> 32 -> 32 -> 1, GELU in its tanh form) looks at the stencil of a face and
 // predicts whether the characteristic-wise WENO-5 flux differs from the
 // component-wise one by more than a relative threshold.  The gated FP32 form
 // computes the cheap component-wise flux on every face, evaluates the MLP on
@@ -66,9 +66,21 @@ __device__ __forceinline__ void mma16816(float d[4], const uint32_t a[4], const 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form, 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))) (Hendrycks &
+// Gimpel 2016), on the special-function unit's tanh (tanh.approx.f32, ~2^-11 relative)
+__device__ __forceinline__ float tanh_fast(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu(float x) {
+    const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+    return 0.5f * x * (1.0f + tanh_fast(k0 * (x + k1 * x * x * x)));
+}
 __device__ __forceinline__ float gelu_grad(float x) {
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * __expf(-0.5f * x * x);
+    const float k0 = 0.7978845608028654f, k1 = 0.044715f;
+    float t = tanh_fast(k0 * (x + k1 * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * k0 * (1.0f + 3.0f * k1 * x * x);
 }
 
 // smem copy of the network: bf16 weight tiles (row = output unit), FP32 vectors
@@ -217,16 +229,17 @@ __device__ __forceinline__ void face_features(const T rho[6], const T p[6], cons
             d[s] = x - mean[v];
             mx = fmaxf(mx, fabsf(d[s]));
         }
-        float inv = 1.f / (mx + scale[v] + 1e-30f);
+        float inv = __fdividef(1.f, mx + scale[v] + 1e-30f);
 #pragma unroll
         for (int s = 0; s < 6; s++) feat[6 * v + s] = d[s] * inv;
     }
     float b0, b1, b2;
     weno_betas<float>(float(rho[0]), float(rho[1]), float(rho[2]), float(rho[3]), float(rho[4]), b0, b1, b2);
     float den = b0 + b1 + b2 + (1e-3f * mr) * (1e-3f * mr) + 1e-30f;
-    feat[18] = b0 / den;
-    feat[19] = b1 / den;
-    feat[20] = b2 / den;
+    float iden = __fdividef(1.f, den);
+    feat[18] = b0 * iden;
+    feat[19] = b1 * iden;
+    feat[20] = b2 * iden;
 }
 
 // rho, p and u_n of the 6-cell stencil of a face

@@ -42,6 +42,7 @@ FORMS = {
     "fp64_char": (2, 0, 0, "f64"),
     "fp64_comp": (1, 0, 0, "f64"),
     "fp32_char": (2, 1, 0, "f32 (f64 RK3 accumulation and reductions)"),
+    "fp32_comp": (1, 1, 0, "f32 (f64 RK3 accumulation and reductions)"),
     "fp32_sensor": (2, 1, 1, "f32 + bf16 sensor (f64 RK3 accumulation and reductions)"),
 }
 
@@ -54,7 +55,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="cells per axis of the shear-layer box")
     ap.add_argument("--form", default="fp64_char", choices=sorted(FORMS))
-    ap.add_argument("--also", default="fp64_comp,fp32_char",
+    ap.add_argument("--also", default="fp64_comp,fp32_char,fp32_comp,fp32_sensor",
                     help="extra forms timed after the headline (comma list, '' for none)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -233,10 +234,20 @@ def main():
     # exactly the library's kernels (torch's default stream is the legacy NULL stream)
     stream = torch.cuda.Stream()
 
+    sensor_w, sensor_info = None, None
+
     def time_form(form, steps, warmup, sample_clocks=False):
+        nonlocal sensor_w, sensor_info
         pf = workload_params(pkg, n, form)
+        if FORMS[form][2] and sensor_w is None:
+            sensor_mod = importlib.import_module("3dnssolver_b200.sensor")
+            X, y = sensor_mod.default_training_set()
+            sensor_w, sensor_info = sensor_mod.train(X, y, seed=0)
+            del X, y
         s = pkg.Solver(pf)
         s.set_stream(stream.cuda_stream)
+        if FORMS[form][2]:
+            s.set_sensor_weights(sensor_w)
         s.upload_primitive(W0)
         s.advance(warmup)
         torch.cuda.synchronize()
@@ -273,8 +284,11 @@ def main():
     fx_faces = (n + 1) * n * n
     face_bytes = cells * 80 + fx_faces * 5 * elem
     upd_bytes = cells * (3 * 40) + 3 * fx_faces * 5 * elem + cells * 40
+    # a fused stage reads U_in and U0 and writes U_out: 120 B per cell (the third stage
+    # also writes the next step's U0; the common 120 B/cell-stage unit is kept)
     alg = {"face_x": face_bytes, "face_y": face_bytes, "face_z": face_bytes, "update": upd_bytes,
-           "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120}
+           "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120,
+           "stage_fused": cells * 120}
     per_launch_ms = prof[dom] / (1 if dom == "step_begin" else 3)
     peaks = {}
     try:
@@ -283,8 +297,9 @@ def main():
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": f"k_face_flux ({dom}, {args.form})" if dom.startswith("face")
-                else dom, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+    kname = {"stage_fused": f"k_stage_fused ({args.form})"}.get(
+        dom, f"k_face_flux ({dom}, {args.form})" if dom.startswith("face") else dom)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4), "traffic": None,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": alg[dom], "launch_ms": round(per_launch_ms, 4),
@@ -311,17 +326,36 @@ def main():
            "steps": args.e2e_steps, "api": "ns_time_step (TimeScheme::step drop-in), pinned host W"}
     s.close()
 
-    # extra forms on the same workload (same timing rules)
+    # extra forms on the same workload (same timing rules); every form advances the
+    # same initial state by warmup + steps steps, so their states compare with the
+    # headline form's: relative L2 error per conserved field against it
+    g3 = slice(3, -3)
     forms = {args.form: {"value": value, "ms_per_step": ms_max / args.steps}}
+    U_ref = None
+    if args.also:
+        s0 = pkg.Solver(p)
+        s0.upload_primitive(W0)
+        s0.advance(args.warmup + args.steps)
+        U_ref = s0.download_conservative()[g3, g3, g3]
+        s0.close()
+    names = ["rho", "rhoE", "rhou", "rhov", "rhow"]
     for f in [x for x in args.also.split(",") if x and x != args.form]:
         try:
-            s2, ms2, _, _, _ = time_form(f, args.steps, args.warmup)
+            s2, ms2, l2, _, d2 = time_form(f, args.steps, args.warmup)
+            U2 = s2.download_conservative()[g3, g3, g3]
             s2.close()
             ms2 = max_over_ranks(ms2)
+            num = np.sqrt(((U2 - U_ref) ** 2).reshape(-1, 5).sum(0))
+            den = np.sqrt((U_ref ** 2).reshape(-1, 5).sum(0))
             forms[f] = {"value": world * cells * 3 * args.steps / (ms2 / 1000.0),
-                        "ms_per_step": ms2 / args.steps}
+                        "ms_per_step": ms2 / args.steps, "gpu_launches": l2,
+                        "rel_l2_vs_" + args.form: {k: float(v) for k, v in zip(names, num / den)}}
+            if FORMS[f][2]:
+                forms[f]["sensor_fraction"] = d2["sensor_fraction"]
+                forms[f]["sensor_training"] = sensor_info
         except Exception as e:
             forms[f] = {"error": str(e)}
+    del U_ref
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

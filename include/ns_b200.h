@@ -159,7 +159,7 @@ NS_API ns_status ns_synchronize(ns_ctx* ctx);
 NS_API ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
 /* Kernel classes timed by ns_profile_step */
 enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FACE_Y = 3,
-       NS_PROF_FACE_Z = 4, NS_PROF_UPDATE = 5, NS_PROF_N = 6 };
+       NS_PROF_FACE_Z = 4, NS_PROF_UPDATE = 5, NS_PROF_STAGE_FUSED = 6, NS_PROF_N = 7 };
 /* Runs one time step of the device-resident state with CUDA events recorded
  * between its kernels on the context's stream; ms[c] receives the device time
  * of kernel class c summed over the step (n >= NS_PROF_N). */

@@ -1,6 +1,6 @@
 """CPU restatement of the learned face sensor (TEST INFRASTRUCTURE ONLY).
 
-numpy FP64 forward/backward of the 21 -> 32 -> 32 -> 1 GELU network and of its
+numpy FP64 forward/backward of the 21 -> 32 -> 32 -> 1 GELU (tanh form) network and of its
 input features, used to check the GPU's BF16 tensor-core kernels (gradients,
 logits) and the feature extraction.  No reference counterpart exists: the
 sensor is an extension of the reference path, so this restatement is the
@@ -9,7 +9,6 @@ oracle for it (parity against it is "unpinned" by the reference).
 import math
 
 import numpy as np
-from scipy.special import erf
 
 NF, NH, NP = 21, 32, 2145
 OFF_W1, OFF_B1, OFF_W2, OFF_B2, OFF_W3, OFF_B3 = 0, 1024, 1056, 2080, 2112, 2144
@@ -22,12 +21,17 @@ def unpack(w):
             w[OFF_W3:OFF_B3], w[OFF_B3])
 
 
+K0, K1 = math.sqrt(2.0 / math.pi), 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / math.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel 2016), as the GPU evaluates it."""
+    return 0.5 * x * (1.0 + np.tanh(K0 * (x + K1 * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2 * math.pi)
+    t = np.tanh(K0 * (x + K1 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * K0 * (1.0 + 3.0 * K1 * x * x)
 
 
 def forward(X, w):

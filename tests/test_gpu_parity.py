@@ -117,8 +117,10 @@ def test_time_steps_match_oracle(oracle, conv, order, bc, weights):
     _assert_close(Ug, Uo, what="U")
 
 
-def test_device_resident_advance_equals_host_steps(oracle):
-    p = pkg.make_params(16, 16, 16, convection=2, diffusion_order=2, bc=(P, P, P), mu=0.01, cfl=0.4)
+@pytest.mark.parametrize("prec", [pkg.PREC_FP64, pkg.PREC_FP32])
+def test_device_resident_advance_equals_host_steps(oracle, prec):
+    p = pkg.make_params(16, 16, 16, convection=2, diffusion_order=2, bc=(P, P, P), mu=0.01, cfl=0.4,
+                        precision=prec)
     W0 = wl.random_field(p, seed=3, smooth=True)
     with pkg.Solver(p) as s:
         s.upload_primitive(W0)
@@ -129,13 +131,16 @@ def test_device_resident_advance_equals_host_steps(oracle):
     with pkg.Solver(p) as s:
         Wh, Uh = W0.copy(), s.new_array()
         dts = [s.time_step(Wh, Uh) for _ in range(5)]
-    np.testing.assert_array_equal(interior(Wd), interior(Wh))
-    np.testing.assert_array_equal(interior(Ud), interior(Uh))
+    # the two routes run the same arithmetic; a fused third stage forms the next
+    # step's start in registers, so they may differ by rounding
+    _assert_close(Wd, Wh, what="device-resident vs host steps (W)")
+    _assert_close(Ud, Uh, what="device-resident vs host steps (U)")
     assert diag["steps"] == 5
-    assert diag["dt"] == dts[-1]
+    assert diag["dt"] == pytest.approx(dts[-1], rel=1e-13)
     np.testing.assert_allclose(diag["time"], sum(dts), rtol=1e-14)
-    Wo, Uo, dto = oracle.run(p, W0, 5)
-    _assert_close(Wd, Wo, what="W after 5 steps")
+    if prec == pkg.PREC_FP64:
+        Wo, Uo, dto = oracle.run(p, W0, 5)
+        _assert_close(Wd, Wo, what="W after 5 steps")
 
 
 def test_compute_dt_matches_reference(oracle):
@@ -193,3 +198,64 @@ def test_fp32_form_close_to_fp64(oracle):
     err = rel_l2(interior(U32), interior(Uo))
     assert (err[[0, 1]] <= 1e-5).all(), err
     assert (err <= 1e-3).all(), err
+
+
+PHYS_CASES = [
+    ((12, 10, 8), 1, 2, (P, P, P), 3),
+    ((12, 10, 8), 2, 4, (N, P, N), 3),
+    ((10, 9, 11), 2, 6, (N, N, N), 3),
+    ((9, 11, 1), 2, 2, (P, N, P), 2),
+]
+
+
+@pytest.mark.parametrize("shape,conv,order,bc,dim", PHYS_CASES)
+@pytest.mark.parametrize("terms", [1, 2, 3])
+def test_physical_semantics_rhs_matches_oracle(oracle, shape, conv, order, bc, dim, terms):
+    """NS_SEM_PHYSICAL (no reference counterpart) against the oracle's restatement."""
+    p = pkg.make_params(*shape, dim=dim, convection=conv, diffusion_order=order, bc=bc, mu=0.03,
+                        L=(1.0, 1.3, 0.7), semantics=pkg.SEM_PHYSICAL)
+    W = wl.random_field(p, seed=sum(shape) + order, smooth=False)
+    with pkg.Solver(p) as s:
+        R = s.rhs(W, terms=terms)
+    Ro = oracle.rhs(p, W, terms=terms)
+    err = rel_l2(interior(R), interior(Ro))
+    ok = np.where(np.sqrt((interior(Ro) ** 2).reshape(-1, 5).sum(0)) == 0,
+                  np.abs(interior(R)).reshape(-1, 5).max(0) == 0, err <= TOL)
+    assert ok.all(), f"rel L2 per field {err}"
+
+
+def test_physical_semantics_steps_match_oracle(oracle):
+    p = pkg.make_params(14, 12, 10, convection=2, diffusion_order=4, bc=(N, P, P), mu=0.02, cfl=0.4,
+                        semantics=pkg.SEM_PHYSICAL)
+    W0 = wl.random_field(p, seed=19, smooth=False)
+    Wo, Uo, dto = oracle.run(p, W0, 3)
+    with pkg.Solver(p) as s:
+        Wg, Ug = W0.copy(), s.new_array()
+        dts = [s.time_step(Wg, Ug) for _ in range(3)]
+    np.testing.assert_allclose(dts, dto, rtol=1e-13)
+    _assert_close(Ug, Uo, what="U (physical semantics)")
+
+
+@pytest.mark.parametrize("conv,order,bc,weights,dim", [
+    (1, 2, (P, P, P), 0, 3), (2, 4, (N, P, P), 0, 3), (2, 6, (N, N, N), 1, 3), (2, 2, (P, N, P), 0, 2),
+])
+def test_fp32_fused_stage_matches_fp32_unfused(conv, order, bc, weights, dim):
+    """The fused FP32 stage kernel (reference semantics) keeps FP32 accuracy against
+    the FP64 path (unfused kernels) on every boundary type, CD order and 2D."""
+    shape = (20, 18, 16) if dim == 3 else (20, 18, 1)
+    kw = dict(dim=dim, convection=conv, diffusion_order=order, bc=bc, weights=weights, mu=0.02,
+              cfl=0.3, precision=pkg.PREC_FP32)
+    p = pkg.make_params(*shape, **kw)
+    W0 = wl.random_field(p, seed=13, smooth=False)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(3)
+        Uf = s.download_conservative()
+    # the FP64 oracle judges both at FP32 accuracy
+    p64 = pkg.make_params(*shape, **dict(kw, precision=pkg.PREC_FP64))
+    with pkg.Solver(p64) as s:
+        s.upload_primitive(W0)
+        s.advance(3)
+        U64 = s.download_conservative()
+    err = rel_l2(interior(Uf), interior(U64))
+    assert (err[[0, 1]] <= 2e-6).all(), err
