@@ -193,6 +193,22 @@ def reference_arm(args):
 
 
 # ---------------------------------------------------------------------------
+# replicas: one rank per GPU, each advancing its own copy of the workload
+
+def max_over_ranks(x, dist=None, device="cuda"):
+    """Maximum of a per-rank float over all ranks (the job's time is its slowest rank)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, cells, steps, ms_max):
+    """Whole-job cell-updates/s per RK3 stage: every rank advanced `cells` cells `steps` steps."""
+    return world * cells * 3 * steps / (ms_max / 1000.0)
+
 
 def main():
     args = parse()
@@ -217,12 +233,8 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def rank_max(x):
+        return max_over_ranks(x, dist)
 
     pkg = importlib.import_module("3dnssolver_b200")
     wl = importlib.import_module("3dnssolver_b200.workloads")
@@ -270,8 +282,8 @@ def main():
         return s, ms, launches, clocks, diag
 
     s, ms, launches, clocks, diag = time_form(args.form, args.steps, args.warmup, sample_clocks=True)
-    ms_max = max_over_ranks(ms)
-    value = world * cells * 3 * args.steps / (ms_max / 1000.0)
+    ms_max = rank_max(ms)
+    value = job_rate(world, cells, args.steps, ms_max)
 
     # per-kernel device times of one step (events between kernels on the same stream)
     profs = [s.profile_step() for _ in range(3)]
@@ -320,8 +332,8 @@ def main():
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e = {"value": world * cells * 3 * args.e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
+    e2e_ms = rank_max(e0.elapsed_time(e1))
+    e2e = {"value": job_rate(world, cells, args.e2e_steps, e2e_ms), "unit": UNIT,
            "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Wh.nbytes),
            "steps": args.e2e_steps, "api": "ns_time_step (TimeScheme::step drop-in), pinned host W"}
     s.close()
@@ -344,10 +356,10 @@ def main():
             s2, ms2, l2, _, d2 = time_form(f, args.steps, args.warmup)
             U2 = s2.download_conservative()[g3, g3, g3]
             s2.close()
-            ms2 = max_over_ranks(ms2)
+            ms2 = rank_max(ms2)
             num = np.sqrt(((U2 - U_ref) ** 2).reshape(-1, 5).sum(0))
             den = np.sqrt((U_ref ** 2).reshape(-1, 5).sum(0))
-            forms[f] = {"value": world * cells * 3 * args.steps / (ms2 / 1000.0),
+            forms[f] = {"value": job_rate(world, cells, args.steps, ms2),
                         "ms_per_step": ms2 / args.steps, "gpu_launches": l2,
                         "rel_l2_vs_" + args.form: {k: float(v) for k, v in zip(names, num / den)}}
             if FORMS[f][2]:

@@ -17,6 +17,11 @@
 //   MODE dt    : TimeScheme::set_dt on the input W; prints the dt
 //   MODE bench : steps= timed TimeScheme::step calls after warmup= untimed ones on
 //                a synthetic shear layer (in= optional); prints one JSON line
+//   MODE dropin: (built with NS_WITH_B200) steps= steps of the same state three
+//                ways: the reference TimeScheme with its own operators, the
+//                reference TimeScheme with the B200 operators plugged in through
+//                ns_b200_adapters.hpp, and the B200 GpuTimeScheme; prints the
+//                relative L2 differences of W per field as JSON
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -35,6 +40,9 @@
 #include "grid.hpp"
 #include "params.hpp"
 #include "time_scheme.hpp" // also brings eq_of_state.hpp, whose include guard (EqOfState_hh vs EqOfSTate_hh) admits one inclusion only
+#ifdef NS_WITH_B200
+#include "ns_b200_adapters.hpp"
+#endif
 
 static std::map<std::string, std::string> kv;
 
@@ -208,6 +216,48 @@ int main(int argc, char** argv) {
         double cells = (double)p.nx * p.ny * p.nz;
         printf("{\"seconds\": %.6f, \"steps\": %d, \"cell_updates_per_s\": %.6e, \"dt\": %.17g}\n",
                sec, steps, cells * 3.0 * steps / sec, ts.get_dt());
+    } else if (mode == "dropin") {
+#ifdef NS_WITH_B200
+        int steps = I("steps", 3);
+        Domain dB(p, dec), dC(p, dec);
+        Array4d& WB = dB.get_NS_primitive_array();
+        Array4d& WC = dC.get_NS_primitive_array();
+        memcpy(&WB(0, 0, 0, 0), &W(0, 0, 0, 0), nall * sizeof(double));
+        memcpy(&WC(0, 0, 0, 0), &W(0, 0, 0, 0), nall * sizeof(double));
+        ns_b200::Context gctx(p);
+        ns_b200::GpuConvection gconv(gctx, p.gamma);
+        ns_b200::GpuDiffusion gdiff(gctx, p);
+        ConvectionScheme* gc = conv ? (ConvectionScheme*)&gconv : cs;
+        DiffusionScheme* gd = diff ? (DiffusionScheme*)&gdiff : ds;
+        TimeScheme tsB(p);
+        ns_b200::GpuTimeScheme tsC(gctx);
+        double dtA = 0, dtB = 0, dtC = 0;
+        for (int s = 0; s < steps; s++) {
+            ts.step(domain, grid, comm, cs, ds);
+            tsB.step(dB, grid, comm, gc, gd);
+            tsC.step(dC, grid, comm, gc, gd);
+            dtA = ts.get_dt(); dtB = tsB.get_dt(); dtC = tsC.get_dt();
+        }
+        auto rel = [&](const Array4d& X, int q) {
+            double num = 0, den = 0;
+            for (size_t i = W.i_begin(); i < W.i_end(); i++)
+                for (size_t j = W.j_begin(); j < W.j_end(); j++)
+                    for (size_t k = W.k_begin(); k < W.k_end(); k++) {
+                        double a = X(i, j, k, q), b = W(i, j, k, q);
+                        num += (a - b) * (a - b);
+                        den += b * b;
+                    }
+            return den > 0 ? sqrt(num / den) : sqrt(num);
+        };
+        printf("{\"steps\": %d, \"dt\": [%.17g, %.17g, %.17g], \"operators\": [", steps, dtA, dtB, dtC);
+        for (int q = 0; q < 5; q++) printf("%s%.6e", q ? ", " : "", rel(WB, q));
+        printf("], \"time_scheme\": [");
+        for (int q = 0; q < 5; q++) printf("%s%.6e", q ? ", " : "", rel(WC, q));
+        printf("]}\n");
+#else
+        fprintf(stderr, "built without NS_WITH_B200\n");
+        return 2;
+#endif
     } else {
         fprintf(stderr, "unknown mode %s\n", mode.c_str());
         return 2;
