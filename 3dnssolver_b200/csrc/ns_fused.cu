@@ -1,15 +1,15 @@
 // ns_fused.cu -- one kernel per SSP-RK3 stage (reference semantics).
 //
-// A block owns a TX x TY x TZ tile of interior cells.  It loads the tile's box
-// with 3 ghost layers on every side once, folding each axis by its boundary
-// condition (periodic wrap or Neumann clamp: the single-GPU form of
-// Domain::apply_boundary_conditions + Communicator::communicate,
-// src/domain.cpp:18-28, src/communicator.cpp:6-143), and keeps W = prim(U)
-// (src/eq_of_state.cpp:61-87) in shared memory.  From there it computes the
-// face fluxes of the tile along x, then y, then z into a shared face buffer,
-// accumulating each cell's (f(+) - f(-))/d in the reference's order
+// A block owns a TY x TZ column of cells and marches along x.  Every plane it
+// touches is loaded once with 3 ghost rows and columns, folding each axis by
+// its boundary condition (periodic wrap or Neumann clamp: the single-GPU form
+// of Domain::apply_boundary_conditions + Communicator::communicate,
+// src/domain.cpp:18-28, src/communicator.cpp:6-143), and kept as W = prim(U)
+// (src/eq_of_state.cpp:61-87) in a shared-memory ring of 7 planes.  For each
+// cell it forms the face fluxes along x (carried from cell to cell in
+// registers), y and z, accumulates (f(+) - f(-))/d in the reference's order
 // (Weno5::compute_residual, weno-5.cpp:39-73), adds the centered viscous terms
-// from the same box, and writes U_out = U0 m1 + U_in m2 + R mc dt
+// from the ring, and writes U_out = U0 m1 + U_in m2 + R mc dt
 // (TimeScheme::substep, time_scheme.cpp:72-96).  U_in and U_out are different
 // buffers: neighbouring blocks read U_in's cells as their ghost layers.
 //
@@ -17,7 +17,7 @@
 // CFL minimum (time_scheme.cpp:69, 98-136) and U0 = cons(W) (the W -> U
 // round trip of time_scheme.cpp:124), so a step is three launches.
 //
-// The Lax-Friedrichs split uses U = cons(W) of the boxed W; it differs from
+// The Lax-Friedrichs split uses U = cons(W) of the ring's W; it differs from
 // the stage's U by rounding only.
 #include <cuda_runtime.h>
 
@@ -31,78 +31,63 @@ namespace nsb {
 
 constexpr int FT = 256;  // threads per block
 
+// ---------------------------------------------------------------------------
+// A block marches LX cells along x over a TY x TZ column: 2.1 plane loads per
+// cell (a 3D box tile with the same shared memory needed 7.4 and ran 20%
+// slower on B200), x-face fluxes carried in registers, y- and z-faces of the
+// current plane through small shared face buffers.
+
 template <typename T>
-struct Tile {
-    static constexpr int TX = 4, TY = 4, TZ = 32;  // 512 cells, 2 per thread
-    static constexpr int BX = TX + 6, BY = TY + 6, BZ = TZ + 6;
-    static constexpr int NB = BX * BY * BZ;  // boxed cells
-    static constexpr int NF = (TX + 1) * TY * TZ > TX * TY * (TZ + 1) ? (TX + 1) * TY * TZ
-                                                                      : TX * TY * (TZ + 1);
-    static constexpr int NC = TX * TY * TZ;
+struct MarchTile {
+    static constexpr int TY = 8, TZ = 32, LX = 32;
+    static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
+    static constexpr int RING = 7;
+    static constexpr int NFY = (TY + 1) * TZ, NFZ = TY * (TZ + 1);
     static constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
-    static constexpr size_t smem = (size_t)5 * NB * sizeof(T) + (size_t)5 * NF * sizeof(T) +
-                                   (size_t)5 * NC * sizeof(double);
+    static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) + (size_t)5 * (NFY + NFZ) * sizeof(T);
 };
 
-// faces of the tile along DIR into Fs, then r += (f(+) - f(-)) / d for the owned cells
-template <int DIR, bool CHAR, bool BORGES, typename T>
-__device__ __forceinline__ void fused_face_pass(const T* __restrict__ Ws, T* __restrict__ Fs,
-                                                double* __restrict__ Rs, T gamma, T inv_gm1,
-                                                double inv_d) {
-    using G = Tile<T>;
-    constexpr int FA = G::TX + (DIR == 0), FB = G::TY + (DIR == 1), FC = G::TZ + (DIR == 2);
-    constexpr int NFD = FA * FB * FC;
-    constexpr int step = DIR == 0 ? G::BY * G::BZ : (DIR == 1 ? G::BZ : 1);
-    const T hg = T(0.5) * gamma * inv_gm1;
-    for (int e = threadIdx.x; e < NFD; e += FT) {
-        int fc = e % FC, t = e / FC, fb = t % FB, fa = t / FB;
-        // stencil cell 0 of face f along DIR is tile cell f-3, box coordinate f
-        int bx = fa + (DIR == 0 ? 0 : 3), by = fb + (DIR == 1 ? 0 : 3), bz = fc + (DIR == 2 ? 0 : 3);
-        int base = (bx * G::BY + by) * G::BZ + bz;
-        T fL[5][5], fR[5][5], wa[5], out[5];
-#pragma unroll
-        for (int s = 0; s < 6; s++) {
-            int idx = base + s * step;
-            T w[5], u[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) w[q] = Ws[q * G::NB + idx];
-            // U = cons(W) (eq_of_state.cpp:32-59)
-            u[0] = w[0];
-            u[2] = w[0] * w[2];
-            u[3] = w[0] * w[3];
-            u[4] = w[0] * w[4];
-            u[1] = w[1] * inv_gm1 + T(0.5) * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-            split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
-        }
-        if constexpr (CHAR)
-            face_char<DIR, false, T, BORGES>(fL, fR, wa, gamma, inv_gm1, out);
-        else
-            face_comp<T, BORGES>(fL, fR, out);
-#pragma unroll
-        for (int q = 0; q < 5; q++) Fs[q * G::NF + e] = out[q];
-    }
-    __syncthreads();
-    for (int cidx = threadIdx.x; cidx < G::NC; cidx += FT) {
-        int lk = cidx % G::TZ, t = cidx / G::TZ, lj = t % G::TY, li = t / G::TY;
-        int left = (li * FB + lj) * FC + lk;
-        int right = left + (DIR == 0 ? FB * FC : (DIR == 1 ? FC : 1));
-#pragma unroll
-        for (int q = 0; q < 5; q++)
-            Rs[q * G::NC + cidx] += (double(Fs[q * G::NF + right]) - double(Fs[q * G::NF + left])) * inv_d;
-    }
-    __syncthreads();
+template <typename T>
+__device__ __forceinline__ int ring_slot(int i, int x0) {
+    return (i - x0 + 3) % MarchTile<T>::RING;  // i >= x0 - 3
 }
 
-// centered viscous terms of tile cell (li, lj, lk) from the box (reference semantics):
-// mixed derivatives differentiate first derivatives that are zero outside the
-// interior along a non-periodic axis (centered_diffusion.cpp:22-24)
-template <int H, typename T>
-__device__ __forceinline__ void fused_viscous(const T* __restrict__ Ws, const Consts& c, int nx,
-                                              int ny, int gi, int gj, int li, int lj, int lk,
-                                              T r[5]) {
-    using G = Tile<T>;
-    const int sx = G::BY * G::BZ, sy = G::BZ;
-    const int o = ((li + 3) * G::BY + (lj + 3)) * G::BZ + (lk + 3);
+// one face from a 6-cell stencil in a shared array with stride `step`
+template <int DIR, bool CHAR, bool BORGES, typename T>
+__device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, T gamma,
+                                           T inv_gm1, T out[5]) {
+    const T hg = T(0.5) * gamma * inv_gm1;
+    T fL[5][5], fR[5][5], wa[5];
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+        const T* P = planes[s];
+        int idx = c0 + s * step;
+        T w[5], u[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) w[q] = P[q * fs + idx];
+        u[0] = w[0];
+        u[2] = w[0] * w[2];
+        u[3] = w[0] * w[3];
+        u[4] = w[0] * w[4];
+        u[1] = w[1] * inv_gm1 + T(0.5) * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
+        split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
+    }
+    if constexpr (CHAR)
+        face_char<DIR, false, T, BORGES>(fL, fR, wa, gamma, inv_gm1, out);
+    else
+        face_comp<T, BORGES>(fL, fR, out);
+}
+
+
+// centered viscous terms of the cell at plane i, in-plane index cc, from the
+// ring (reference semantics): mixed derivatives differentiate first
+// derivatives that are zero outside the interior along a non-periodic axis
+// (centered_diffusion.cpp:22-24)
+template <int H, typename T, typename PlaneFn>
+__device__ __forceinline__ void march_viscous(PlaneFn plane, int i, int cc, const Consts& c, int nx,
+                                              int ny, int gi, int gj, T r[5]) {
+    using M = MarchTile<T>;
+    const int sy = M::PZ, fs = M::NP;
     T cx1[2 * H + 1], cy1[2 * H + 1], cxx[2 * H + 1], cyy[2 * H + 1];
 #pragma unroll
     for (int t = 0; t <= 2 * H; t++) {
@@ -111,14 +96,17 @@ __device__ __forceinline__ void fused_viscous(const T* __restrict__ Ws, const Co
         cxx[t] = T(c.ddf[3 - H + t] * c.inv_dx * c.inv_dx);
         cyy[t] = T(c.ddf[3 - H + t] * c.inv_dy * c.inv_dy);
     }
+    const T* P[2 * H + 1];
+#pragma unroll
+    for (int t = 0; t <= 2 * H; t++) P[t] = plane(i + t - H);
     T Dx[4], Dy[4], Dxx[4], Dyy[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) {
         T a1 = 0, b1 = 0, a2 = 0, b2 = 0;
 #pragma unroll
         for (int t = 0; t <= 2 * H; t++) {
-            T wx = Ws[q * G::NB + o + (t - H) * sx];
-            T wy = Ws[q * G::NB + o + (t - H) * sy];
+            T wx = P[t][q * fs + cc];
+            T wy = P[H][q * fs + cc + (t - H) * sy];
             if (t != H) { a1 += wx * cx1[t]; b1 += wy * cy1[t]; }
             a2 += wx * cxx[t];
             b2 += wx * cyy[t];  // d2/dy2 uses the x-stencil (cd-n.cpp:77)
@@ -138,7 +126,7 @@ __device__ __forceinline__ void fused_viscous(const T* __restrict__ Ws, const Co
                 T dx = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * H; t++)
-                    if (t != H) dx += Ws[q * G::NB + o + (s - H) * sy + (t - H) * sx] * cx1[t];
+                    if (t != H) dx += P[t][q * fs + cc + (s - H) * sy] * cx1[t];
                 sxy += dx * cy1[s];
             }
             int ii = gi + s - H;
@@ -146,103 +134,150 @@ __device__ __forceinline__ void fused_viscous(const T* __restrict__ Ws, const Co
                 T dy = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * H; t++)
-                    if (t != H) dy += Ws[q * G::NB + o + (s - H) * sx + (t - H) * sy] * cy1[t];
+                    if (t != H) dy += P[s][q * fs + cc + (t - H) * sy] * cy1[t];
                 syx += dy * cx1[s];
             }
         }
         Dxy[v] = sxy; Dyx[v] = syx;
     }
-    viscous_reference_terms<T>(Dx, Dy, Dxx, Dyy, Dxy, Dyx, Ws[2 * G::NB + o], Ws[3 * G::NB + o],
-                               Ws[1 * G::NB + o], Ws[o], c, r);
+    viscous_reference_terms<T>(Dx, Dy, Dxx, Dyy, Dxy, Dyx, P[H][2 * fs + cc], P[H][3 * fs + cc],
+                               P[H][1 * fs + cc], P[H][cc], c, r);
 }
 
 template <typename T, bool CHAR, bool BORGES, int H, bool LAST>
-__global__ void __launch_bounds__(FT, Tile<T>::MINB)
-    k_stage_fused(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
+__global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
+    k_stage_march(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
                   Consts c, int conv_dims, double m1, double m2, double mc,
                   const unsigned long long* __restrict__ slot, unsigned long long* slot_next,
                   double* clock) {
-    using G = Tile<T>;
+    using M = MarchTile<T>;
     extern __shared__ __align__(16) unsigned char smem[];
-    T* Ws = reinterpret_cast<T*>(smem);
-    T* Fs = Ws + 5 * G::NB;
-    double* Rs = reinterpret_cast<double*>(Fs + 5 * G::NF);
-    const int i0 = blockIdx.z * G::TX, j0 = blockIdx.y * G::TY, k0 = blockIdx.x * G::TZ;
-    // 1. box of W = prim(U_in) at folded positions
-    for (int e = threadIdx.x; e < G::NB; e += FT) {
-        int bz = e % G::BZ, t = e / G::BZ, by = t % G::BY, bx = t / G::BY;
-        int gi = fold(i0 - 3 + bx, b.nx, c.periodic[0]);
-        int gj = fold(j0 - 3 + by, b.ny, c.periodic[1]);
-        int gk = fold(k0 - 3 + bz, b.nz, c.periodic[2]);
-        long long o = b.at(gi + NG, gj + NG, gk + NG);
-        double u[5], w[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) u[q] = Uin[q * b.fstride + o];
-        prim_from_cons(u, c.gm1, w);
-#pragma unroll
-        for (int q = 0; q < 5; q++) Ws[q * G::NB + e] = T(w[q]);
-    }
-    for (int e = threadIdx.x; e < 5 * G::NC; e += FT) Rs[e] = 0.0;
-    __syncthreads();
-    // 2. convective residual, x then y then z
+    T* ring = reinterpret_cast<T*>(smem);  // [RING][5][NP]
+    T* FY = ring + M::RING * 5 * M::NP;    // [5][NFY]
+    T* FZ = FY + 5 * M::NFY;               // [5][NFZ]
+    const int tid = threadIdx.x, ty = tid / M::TZ, tz = tid % M::TZ;
+    const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * M::LX;
+    const int x1 = min(x0 + M::LX, b.nx);
     const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
-    if (conv_dims > 0) {
-        fused_face_pass<0, CHAR, BORGES, T>(Ws, Fs, Rs, gamma, inv_gm1, c.inv_dx);
-        fused_face_pass<1, CHAR, BORGES, T>(Ws, Fs, Rs, gamma, inv_gm1, c.inv_dy);
-        if (conv_dims == 3) fused_face_pass<2, CHAR, BORGES, T>(Ws, Fs, Rs, gamma, inv_gm1, c.inv_dz);
-    }
-    // 3. viscous terms + RK combination for the owned cells
+    auto plane = [&](int i) { return ring + ring_slot<T>(i, x0) * 5 * M::NP; };
+    // W = prim(U_in) of plane i at folded positions
+    auto load_plane = [&](int i) {
+        T* P = plane(i);
+        const int gi = fold(i, b.nx, c.periodic[0]);
+        for (int e = tid; e < M::NP; e += FT) {
+            int py = e / M::PZ, pz = e % M::PZ;
+            int gj = fold(j0 - 3 + py, b.ny, c.periodic[1]);
+            int gk = fold(k0 - 3 + pz, b.nz, c.periodic[2]);
+            long long o = b.at(gi + NG, gj + NG, gk + NG);
+            double u[5], w[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) u[q] = Uin[q * b.fstride + o];
+            prim_from_cons(u, c.gm1, w);
+#pragma unroll
+            for (int q = 0; q < 5; q++) P[q * M::NP + e] = T(w[q]);
+        }
+    };
+    // x-face of this thread's column between cells i and i+1 (stencil i-2..i+3)
+    const int ccol = (ty + 3) * M::PZ + (tz + 3);
+    auto xface = [&](int i, T out[5]) {
+        const T* P[6];
+#pragma unroll
+        for (int s = 0; s < 6; s++) P[s] = plane(i - 2 + s);
+        march_face<0, CHAR, BORGES, T>(P, ccol, 0, M::NP, gamma, inv_gm1, out);
+    };
+    for (int i = x0 - 3; i < x0 + 3; i++) load_plane(i);
+    __syncthreads();
+    T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
+    if (conv_dims > 0) xface(x0 - 1, fxl);
     const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
     const double m3 = mc * dt;
-    if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x) == 0) {
+    if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) {
         clock[0] = dt;
         clock[1] += dt;
     }
+    const int gj = j0 + ty, gk = k0 + tz;
+    const bool own = gj < b.ny && gk < b.nz;
     double best = INFINITY;
-    for (int cidx = threadIdx.x; cidx < G::NC; cidx += FT) {
-        int lk = cidx % G::TZ, t = cidx / G::TZ, lj = t % G::TY, li = t / G::TY;
-        int gi = i0 + li, gj = j0 + lj, gk = k0 + lk;
-        if (gi >= b.nx || gj >= b.ny || gk >= b.nz) continue;
-        double r[5];
+    for (int i = x0; i < x1; i++) {
+        load_plane(i + 3);
+        __syncthreads();
+        const T* Pi = plane(i);
+        if (conv_dims > 0) {
+            xface(i, fxr);
+            // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
+            for (int e = tid; e < M::NFY; e += FT) {
+                int fb = e / M::TZ, cz = e % M::TZ;
+                const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
+                T out[5];
+                march_face<1, CHAR, BORGES, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1, out);
 #pragma unroll
-        for (int q = 0; q < 5; q++) r[q] = Rs[q * G::NC + cidx];
-        if constexpr (H > 0) {
-            T rv[5] = {0, 0, 0, 0, 0};
-            fused_viscous<H, T>(Ws, c, b.nx, b.ny, gi, gj, li, lj, lk, rv);
+                for (int q = 0; q < 5; q++) FY[q * M::NFY + e] = out[q];
+            }
+            if (conv_dims == 3) {
+                for (int e = tid; e < M::NFZ; e += FT) {
+                    int ry = e / (M::TZ + 1), fc = e % (M::TZ + 1);
+                    const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
+                    T out[5];
+                    march_face<2, CHAR, BORGES, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1, out);
 #pragma unroll
-            for (int q = 1; q < 5; q++) r[q] += double(rv[q]);
+                    for (int q = 0; q < 5; q++) FZ[q * M::NFZ + e] = out[q];
+                }
+            }
         }
-        long long o = b.at(gi + NG, gj + NG, gk + NG);
-        double un[5];
+        __syncthreads();
+        if (own) {
+            double r[5] = {0, 0, 0, 0, 0};
+            if (conv_dims > 0) {
 #pragma unroll
-        for (int q = 0; q < 5; q++) {
-            long long a = q * b.fstride + o;
-            un[q] = (U0[a] * m1) + (Uin[a] * m2) + (r[q] * m3);
-            Uout[a] = un[q];
-        }
-        if constexpr (LAST) {
-            // start of the next step: W = prim(U), its CFL minimum, U0 = cons(W)
-            double w[5], u0[5];
-            prim_from_cons(un, c.gm1, w);
-            double d = local_dt(w, c);
-            if (d < best) best = d;
-            cons_from_prim(w, c.inv_gm1, u0);
+                for (int q = 0; q < 5; q++) {
+                    r[q] += (double(fxr[q]) - double(fxl[q])) * c.inv_dx;
+                    r[q] += (double(FY[q * M::NFY + (ty + 1) * M::TZ + tz]) -
+                             double(FY[q * M::NFY + ty * M::TZ + tz])) * c.inv_dy;
+                    if (conv_dims == 3)
+                        r[q] += (double(FZ[q * M::NFZ + ty * (M::TZ + 1) + tz + 1]) -
+                                 double(FZ[q * M::NFZ + ty * (M::TZ + 1) + tz])) * c.inv_dz;
+                }
+            }
+            if constexpr (H > 0) {
+                T rv[5] = {0, 0, 0, 0, 0};
+                march_viscous<H, T>(plane, i, ccol, c, b.nx, b.ny, i, gj, rv);
 #pragma unroll
-            for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u0[q];
+                for (int q = 1; q < 5; q++) r[q] += double(rv[q]);
+            }
+            long long o = b.at(i + NG, gj + NG, gk + NG);
+            double un[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                long long a = q * b.fstride + o;
+                un[q] = (U0[a] * m1) + (Uin[a] * m2) + (r[q] * m3);
+                Uout[a] = un[q];
+            }
+            if constexpr (LAST) {
+                double w[5], u0[5];
+                prim_from_cons(un, c.gm1, w);
+                double d = local_dt(w, c);
+                if (d < best) best = d;
+                cons_from_prim(w, c.inv_gm1, u0);
+#pragma unroll
+                for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u0[q];
+            }
         }
+#pragma unroll
+        for (int q = 0; q < 5; q++) fxl[q] = fxr[q];
+        __syncthreads();
     }
     if constexpr (LAST) block_min_to(best, slot_next);
 }
 
 template <typename T, bool CHAR, bool BORGES, int H, bool LAST>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
-    using G = Tile<T>;
-    auto kern = k_stage_fused<T, CHAR, BORGES, H, LAST>;
+    using M = MarchTile<T>;
+    auto kern = k_stage_march<T, CHAR, BORGES, H, LAST>;
     // the attribute is per device; setting it on every launch keeps multi-device use correct
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::smem);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.b.nz + G::TZ - 1) / G::TZ, (a.b.ny + G::TY - 1) / G::TY, (a.b.nx + G::TX - 1) / G::TX);
-    kern<<<grid, FT, G::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
+    dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + M::LX - 1) / M::LX);
+    kern<<<grid, FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
                                    a.slot_next, a.clock);
     return cudaGetLastError();
 }
