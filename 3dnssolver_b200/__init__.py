@@ -79,6 +79,7 @@ def load_library():
         "ns_sensor_gradients": ([C, C, ctypes.c_int, ctypes.c_float, fp, fp, fp, C], st),
         "ns_sensor_predict": ([C, ctypes.c_longlong, fp, C, C], st),
         "ns_set_sensor_weights": ([C, fp], st),
+        "ns_fma_peak": ([ctypes.c_int, dp], st),
     }
     for name, (args, res) in protos.items():
         f = getattr(L, name)
@@ -109,6 +110,13 @@ def _fptr(a):
 
 SENSOR_FEATURES = 21
 SENSOR_NPARAMS = 2145
+
+
+def fma_peak(fp64=True):
+    """Measured FMA throughput of the current device, TFLOP/s (2 flops per FMA)."""
+    t = ctypes.c_double()
+    _check(load_library().ns_fma_peak(1 if fp64 else 0, ctypes.byref(t)), "ns_fma_peak")
+    return t.value
 
 
 def sensor_init(seed):

@@ -710,6 +710,41 @@ ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
 
 long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+ns_status ns_fma_peak(int fp64, double* tflops) {
+    if (!tflops) return fail(NS_ERR_INVALID_ARG, "tflops is NULL");
+    int dev = 0, sms = 0;
+    NS_CUDA(cudaGetDevice(&dev));
+    NS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = sms * 8, iters = 4096;
+    void* sink = nullptr;
+    NS_CUDA(cudaMalloc(&sink, 16));
+    cudaStream_t s;
+    cudaEvent_t e0, e1;
+    NS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    NS_CUDA(cudaEventCreate(&e0));
+    NS_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    ns_status st = NS_OK;
+    for (int r = 0; r < 5 && st == NS_OK; r++) {
+        cudaEventRecord(e0, s);
+        if (launch_fma_probe(fp64 != 0, blocks, iters, sink, s) != cudaSuccess)
+            st = fail(NS_ERR_CUDA, "FMA probe launch failed");
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = fail(NS_ERR_CUDA, "FMA probe failed");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (r > 0 && ms < best) best = ms;  // the first run warms up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    cudaFree(sink);
+    if (st != NS_OK) return st;
+    const double flops = 2.0 * 8.0 * iters * 256.0 * blocks;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return NS_OK;
+}
+
 ns_status ns_set_sensor_weights(ns_ctx* ctx, const float* w) {
     if (!ctx || !w) return fail(NS_ERR_INVALID_ARG, "ctx and w must be non-NULL");
     if (!ctx->sensor) return fail(NS_ERR_INVALID_ARG, "the context was created without the sensor (params.sensor = 0)");

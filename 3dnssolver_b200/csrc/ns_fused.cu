@@ -32,14 +32,21 @@ namespace nsb {
 constexpr int FT = 256;  // threads per block
 
 // ---------------------------------------------------------------------------
-// A block marches LX cells along x over a TY x TZ column: 2.1 plane loads per
+// A block marches LX cells along x over a TY x TZ column: 2.2 plane loads per
 // cell (a 3D box tile with the same shared memory needed 7.4 and ran 20%
 // slower on B200), x-face fluxes carried in registers, y- and z-faces of the
 // current plane through small shared face buffers.
 
+// TY x TZ = 8 x 32 cells per plane, one per thread.  A 7-row tile (one round
+// per face pass instead of two for the 288 y- and 264 z-faces) measured the
+// same on B200 (+2.6% component-wise, -3% characteristic), so the plane of 8
+// rows stays; NS_MARCH_TY selects it at build time.
+#ifndef NS_MARCH_TY
+#define NS_MARCH_TY 8
+#endif
 template <typename T>
 struct MarchTile {
-    static constexpr int TY = 8, TZ = 32, LX = 32;
+    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = 32;
     static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
     static constexpr int RING = 7;
     static constexpr int NFY = (TY + 1) * TZ, NFZ = TY * (TZ + 1);
@@ -188,7 +195,8 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
     for (int i = x0 - 3; i < x0 + 3; i++) load_plane(i);
     __syncthreads();
     T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
-    if (conv_dims > 0) xface(x0 - 1, fxl);
+    const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
+    if (conv_dims > 0 && row) xface(x0 - 1, fxl);
     const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
     const double m3 = mc * dt;
     if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) {
@@ -196,14 +204,14 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
         clock[1] += dt;
     }
     const int gj = j0 + ty, gk = k0 + tz;
-    const bool own = gj < b.ny && gk < b.nz;
+    const bool own = row && gj < b.ny && gk < b.nz;
     double best = INFINITY;
     for (int i = x0; i < x1; i++) {
         load_plane(i + 3);
         __syncthreads();
         const T* Pi = plane(i);
         if (conv_dims > 0) {
-            xface(i, fxr);
+            if (row) xface(i, fxr);
             // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
             for (int e = tid; e < M::NFY; e += FT) {
                 int fb = e / M::TZ, cz = e % M::TZ;

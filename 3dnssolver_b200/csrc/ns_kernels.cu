@@ -639,3 +639,31 @@ void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* 
 }
 
 }  // namespace nsb
+
+// ---------------------------------------------------------------------------
+// FMA throughput probe: the measured denominator of the compute roofline.
+// Every thread runs 8 independent FMA chains (enough to cover the pipe's
+// latency); the result is written only if it is NaN so the work is kept.
+namespace nsb {
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_probe(int iters, T seed, T* sink) {
+    T a[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) a[c] = seed + T(threadIdx.x + c);
+    const T m = T(0.999999), k = T(1e-7);
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int c = 0; c < 8; c++) a[c] = a[c] * m + k;
+    }
+    T s = a[0] + a[1] + a[2] + a[3] + a[4] + a[5] + a[6] + a[7];
+    if (s != s) *sink = s;
+}
+
+cudaError_t launch_fma_probe(bool fp64, int blocks, int iters, void* sink, cudaStream_t s) {
+    if (fp64)
+        k_fma_probe<double><<<blocks, 256, 0, s>>>(iters, 1.0, (double*)sink);
+    else
+        k_fma_probe<float><<<blocks, 256, 0, s>>>(iters, 1.0f, (float*)sink);
+    return cudaGetLastError();
+}
+}  // namespace nsb

@@ -46,6 +46,8 @@ struct FusedArgs {
 };
 cudaError_t launch_stage_fused(const FusedArgs& a, cudaStream_t s);
 
+cudaError_t launch_fma_probe(bool fp64, int blocks, int iters, void* sink, cudaStream_t s);
+
 void launch_step_begin(bool from_u, bool phys, double* W, double* U, double* U0, const Box& b,
                        const Consts& c, unsigned long long* slot, cudaStream_t s);
 void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s);

@@ -210,6 +210,90 @@ def job_rate(world, cells, steps, ms_max):
     return world * cells * 3 * steps / (ms_max / 1000.0)
 
 
+# ---------------------------------------------------------------------------
+# rooflines of the dominant kernel
+
+# Floating-point work per unit of each kernel class, counted by ncu on the 128^3
+# shear layer (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}_pred_on.sum
+# divided by the faces or cells of the launch; the counts do not depend on the data):
+# (flop per unit with an FMA as 2, FP instructions per unit, pipe, unit).
+# The fused stage rows are the first two stages; the third adds the next step's
+# start (about 70 FP64 instructions per cell).
+COMPUTE_PER_UNIT = {
+    ("fp64_char", "face_x"): (1325, 953, "fp64", "face"),
+    ("fp64_char", "face_y"): (1325, 953, "fp64", "face"),
+    ("fp64_char", "face_z"): (1318, 946, "fp64", "face"),
+    ("fp64_comp", "face_x"): (965, 729, "fp64", "face"),
+    ("fp64_comp", "face_y"): (965, 729, "fp64", "face"),
+    ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
+    ("fp64_char", "update"): (316, 205, "fp64", "cell"),
+    ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
+    ("fp32_char", "stage_fused"): (4112, 2928, "fp32", "cell"),
+    ("fp32_comp", "stage_fused"): (3022, 2279, "fp32", "cell"),
+}
+# DRAM bytes (read + write) per unit from the same capture; these kernels stream
+# their inputs once at 128^3 and above, so the traffic scales with the units.
+TRAFFIC_PER_UNIT = {
+    ("fp64_char", "face_x"): 120.4, ("fp64_char", "face_y"): 118.6, ("fp64_char", "face_z"): 113.6,
+    ("fp64_comp", "face_x"): 119.7, ("fp64_comp", "face_y"): 118.7, ("fp64_comp", "face_z"): 113.3,
+    ("fp64_char", "update"): 283.7, ("fp64_comp", "update"): 283.7,
+}
+
+
+def profile(s, reps=3):
+    """Mean per-class device ms of one step (events between the kernels)."""
+    profs = [s.profile_step() for _ in range(reps)]
+    return {k: statistics.mean(pr[k] for pr in profs) for k in profs[0]}
+
+
+def rooflines(form, prof, n, peaks, fma):
+    """HBM and compute rooflines of the form's dominant kernel class."""
+    cells = n ** 3
+    dom = max(prof, key=prof.get)
+    launches = 1 if dom == "step_begin" else 3
+    per_launch_ms = prof[dom] / launches
+    # algorithmic bytes: a face-flux launch reads W and U (2 x 5 doubles per cell) and
+    # writes 5 values per face; an update launch reads U, U0 and 3 face arrays and
+    # writes U; a fused stage reads U_in and U0 and writes U_out: 120 B per cell (the
+    # third stage also writes the next step's U0; the common 120 B/cell-stage unit is kept)
+    elem = 4 if FORMS[form][1] == 1 else 8
+    faces = (n + 1) * n * n
+    face_bytes = cells * 80 + faces * 5 * elem
+    alg = {"face_x": face_bytes, "face_y": face_bytes, "face_z": face_bytes,
+           "update": cells * (3 * 40) + 3 * faces * 5 * elem + cells * 40,
+           "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120,
+           "stage_fused": cells * 120}
+    kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})"}.get(
+        dom, f"k_face_flux ({dom}, {form})" if dom.startswith("face") else dom)
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
+    units = faces if dom.startswith("face") else cells
+    tpu = TRAFFIC_PER_UNIT.get((form, dom))
+    hbm = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+           "frac": round(achieved / hbm_peak, 4),
+           "traffic": round(tpu * units) if tpu else None,
+           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit at 128^3, "
+                             "scaled by the units of this launch" if tpu else None,
+           "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s",
+           "algorithmic_bytes_per_launch": alg[dom], "launch_ms": round(per_launch_ms, 4)}
+    comp = None
+    row = COMPUTE_PER_UNIT.get((form, dom))
+    if row:
+        flop_u, inst_u, pipe, unit = row
+        peak = fma[pipe]
+        tflops = flop_u * units / (per_launch_ms / 1000.0) / 1e12
+        # FP instructions against the FMA issue rate (peak / 2 flops): a multiply or add
+        # takes the same pipe slot as an FMA, so this is the pipe's busy fraction
+        inst_rate = inst_u * units / (per_launch_ms / 1000.0) / 1e12
+        comp = {"bound": pipe, "kernel": kname, "achieved": round(tflops, 2), "peak": round(peak, 2),
+                "unit": "TFLOP/s", "frac": round(tflops / peak, 4),
+                "pipe_frac": round(inst_rate / (peak / 2.0), 4),
+                "peak_source": f"measured now: ns_fma_peak ({pipe} FMA chains on every SM)",
+                "flop_per_" + unit: flop_u, "fp_inst_per_" + unit: inst_u}
+        hbm["note"] = f"{pipe}-pipe bound: see compute_roofline"
+    return hbm, comp
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -266,6 +350,12 @@ def main():
         clk = ClockSampler(local) if sample_clocks else None
         if clk:
             clk.start()
+            # untimed steps for about a second, so that the sampler (200 ms period)
+            # sees the GPU under this load right up to and through the timed region
+            t0 = time.time()
+            while time.time() - t0 < 1.0:
+                s.advance(2)
+                torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
         l0 = s.launches
@@ -286,36 +376,14 @@ def main():
     value = job_rate(world, cells, args.steps, ms_max)
 
     # per-kernel device times of one step (events between kernels on the same stream)
-    profs = [s.profile_step() for _ in range(3)]
-    prof = {k: statistics.mean(pr[k] for pr in profs) for k in profs[0]}
-    faces_ms = {k: v for k, v in prof.items() if k.startswith("face_")}
-    dom = max(prof, key=prof.get)
-    # algorithmic bytes: a face-flux launch reads W and U (2 x 5 doubles per cell) and
-    # writes 5 doubles per face; an update launch reads U, U0 and 3 face arrays and writes U
-    elem = 4 if FORMS[args.form][1] == 1 else 8
-    fx_faces = (n + 1) * n * n
-    face_bytes = cells * 80 + fx_faces * 5 * elem
-    upd_bytes = cells * (3 * 40) + 3 * fx_faces * 5 * elem + cells * 40
-    # a fused stage reads U_in and U0 and writes U_out: 120 B per cell (the third stage
-    # also writes the next step's U0; the common 120 B/cell-stage unit is kept)
-    alg = {"face_x": face_bytes, "face_y": face_bytes, "face_z": face_bytes, "update": upd_bytes,
-           "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120,
-           "stage_fused": cells * 120}
-    per_launch_ms = prof[dom] / (1 if dom == "step_begin" else 3)
+    prof = profile(s)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
-    kname = {"stage_fused": f"k_stage_fused ({args.form})"}.get(
-        dom, f"k_face_flux ({dom}, {args.form})" if dom.startswith("face") else dom)
-    roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "traffic": None,
-                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s",
-                "algorithmic_bytes_per_launch": alg[dom], "launch_ms": round(per_launch_ms, 4),
-                "note": "FP64 characteristic-wise WENO is FP64-pipe bound; see compute_roofline"}
+    fma = {"fp64": pkg.fma_peak(True), "fp32": pkg.fma_peak(False)}
+    roofline, compute_roofline = rooflines(args.form, prof, n, peaks, fma)
 
     # end to end through the C ABI with host buffers: ns_time_step uploads W from pinned
     # host memory, runs the step and downloads W every step
@@ -355,13 +423,15 @@ def main():
         try:
             s2, ms2, l2, _, d2 = time_form(f, args.steps, args.warmup)
             U2 = s2.download_conservative()[g3, g3, g3]
+            hbm2, comp2 = rooflines(f, profile(s2), n, peaks, fma)
             s2.close()
             ms2 = rank_max(ms2)
             num = np.sqrt(((U2 - U_ref) ** 2).reshape(-1, 5).sum(0))
             den = np.sqrt((U_ref ** 2).reshape(-1, 5).sum(0))
             forms[f] = {"value": job_rate(world, cells, args.steps, ms2),
                         "ms_per_step": ms2 / args.steps, "gpu_launches": l2,
-                        "rel_l2_vs_" + args.form: {k: float(v) for k, v in zip(names, num / den)}}
+                        "rel_l2_vs_" + args.form: {k: float(v) for k, v in zip(names, num / den)},
+                        "roofline": hbm2, "compute_roofline": comp2}
             if FORMS[f][2]:
                 forms[f]["sensor_fraction"] = d2["sensor_fraction"]
                 forms[f]["sensor_training"] = sensor_info
@@ -384,7 +454,7 @@ def main():
             "config": {"workload": workload_name(n, args.form), "grid": [n, n, n], "form": args.form,
                        "l2": "no flush: device state 2.9 GB > 126 MB L2",
                        "parallelism": f"{world} independent replica(s), no data-path collective"},
-            "roofline": roofline,
+            "roofline": roofline, "compute_roofline": compute_roofline,
             "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "forms": forms,

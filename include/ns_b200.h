@@ -225,6 +225,10 @@ NS_API ns_status ns_set_sensor_weights(ns_ctx* ctx, const float* w);
 #define NS_NOALLOC_SCRATCH_BYTES (32u << 20)
 NS_API ns_status ns_convection_solve_noalloc(const ns_params* p, const double* W, const double* U,
                                              double* R, void* cuda_stream);
+/* Measured FMA throughput of the current device in TFLOP/s (2 flops per FMA):
+ * fp64 = 1 for double, 0 for float.  The denominator of the compute roofline
+ * of the FMA-bound WENO kernels (no counterpart in the reference). */
+NS_API ns_status ns_fma_peak(int fp64, double* tflops);
 /* Device kernels launched by this context since creation (for launch accounting). */
 NS_API long long ns_kernel_launches(ns_ctx* ctx);
 
