@@ -24,6 +24,7 @@
 #include "ns_common.cuh"
 #include "ns_eos.cuh"
 #include "ns_face.cuh"
+#include "ns_face_f32x2.cuh"
 #include "ns_kernels.h"
 #include "ns_viscous.cuh"
 
@@ -63,6 +64,10 @@ __device__ __forceinline__ int ring_slot(int i, int x0) {
 template <int DIR, bool CHAR, bool BORGES, typename T>
 __device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, T gamma,
                                            T inv_gm1, T out[5]) {
+    if constexpr (sizeof(T) == 4) {
+        face_f32x2<DIR, CHAR, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
+        return;
+    }
     const T hg = T(0.5) * gamma * inv_gm1;
     T fL[5][5], fR[5][5], wa[5];
 #pragma unroll
