@@ -76,44 +76,60 @@ __device__ __forceinline__ float weno_f32x2(f2 a, f2 b, f2 c, f2 d, f2 e) {
     return __fdividef(num.x, den.x) + __fdividef(num.y, den.y);
 }
 
+// Half the Euler flux along DIR (half_flux) and U = cons(W) of two cells at once.
+template <int DIR>
+__device__ __forceinline__ void cell_pair_f32x2(const f2 w[5], float hg, float inv_gm1, f2 u[5], f2 f[5]) {
+    const f2 half = sp2(0.5f);
+    const f2 hr = mul2(half, w[0]);
+    const f2 hrq = mul2(hr, w[2 + DIR]);
+    const f2 ke = fma2(w[2], w[2], fma2(w[3], w[3], mul2(w[4], w[4])));
+    u[0] = w[0];
+    u[1] = fma2(w[1], sp2(inv_gm1), mul2(hr, ke));
+    u[2] = mul2(w[0], w[2]);
+    u[3] = mul2(w[0], w[3]);
+    u[4] = mul2(w[0], w[4]);
+    f[0] = hrq;
+    f[1] = mul2(w[2 + DIR], fma2(sp2(hg), w[1], mul2(mul2(sp2(0.5f), hr), ke)));
+    const f2 hp = mul2(half, w[1]);
+    f[2] = DIR == 0 ? fma2(hrq, w[2], hp) : mul2(hrq, w[2]);
+    f[3] = DIR == 1 ? fma2(hrq, w[3], hp) : mul2(hrq, w[3]);
+    f[4] = DIR == 2 ? fma2(hrq, w[4], hp) : mul2(hrq, w[4]);
+}
+
 // Packed stencil of one face: P[q][k] = (fL_q of cell k, fR_q of cell 5-k),
-// cells 0..5 = a-2..a+3, from W at the 6 cells.  U = cons(W); half the Euler
-// flux (division free, see half_flux); Lax-Friedrichs split with alpha = 3.
-// wa receives the face average of W (cells 2 and 3).
+// cells 0..5 = a-2..a+3, from W at the 6 cells: cells k and 5-k share a lane
+// pair for U = cons(W) and half the Euler flux (division free); Lax-Friedrichs
+// split with alpha = 3.  wa receives the face average of W (cells 2 and 3).
 template <int DIR, bool CHAR>
 __device__ __forceinline__ void stencil_f32x2(const float* const* planes, int c0, int step, int fs,
                                               float gamma, float inv_gm1, f2 P[5][5], float wa[5]) {
     const float hg = 0.5f * gamma * inv_gm1;
-    float u[6][5], f[6][5];
+    f2 U[3][5], F[3][5];
 #pragma unroll
-    for (int s = 0; s < 6; s++) {
-        const float* Q = planes[s];
-        const int idx = c0 + s * step;
-        float w[5];
+    for (int k = 0; k < 3; k++) {
+        const float* A = planes[k];
+        const float* B = planes[5 - k];
+        const int ia = c0 + k * step, ib = c0 + (5 - k) * step;
+        f2 w[5];
 #pragma unroll
-        for (int q = 0; q < 5; q++) w[q] = Q[q * fs + idx];
-        u[s][0] = w[0];
-        u[s][2] = w[0] * w[2];
-        u[s][3] = w[0] * w[3];
-        u[s][4] = w[0] * w[4];
-        u[s][1] = w[1] * inv_gm1 + 0.5f * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-        half_flux<DIR, float>(w, hg, f[s]);
+        for (int q = 0; q < 5; q++) w[q] = make_float2(A[q * fs + ia], B[q * fs + ib]);
         if constexpr (CHAR) {
-            if (s == 2) {
+            if (k == 2) {
 #pragma unroll
-                for (int q = 0; q < 5; q++) wa[q] = w[q];
-            }
-            if (s == 3) {
-#pragma unroll
-                for (int q = 0; q < 5; q++) wa[q] = 0.5f * (wa[q] + w[q]);
+                for (int q = 0; q < 5; q++) wa[q] = 0.5f * (w[q].x + w[q].y);
             }
         }
+        cell_pair_f32x2<DIR>(w, hg, inv_gm1, U[k], F[k]);
     }
+    const f2 lr = make_float2(1.5f, -1.5f);
 #pragma unroll
-    for (int q = 0; q < 5; q++)
+    for (int q = 0; q < 5; q++) {
 #pragma unroll
-        for (int k = 0; k < 5; k++)
-            P[q][k] = make_float2(fmaf(1.5f, u[k][q], f[k][q]), fmaf(-1.5f, u[5 - k][q], f[5 - k][q]));
+        for (int k = 0; k < 3; k++) P[q][k] = fma2(lr, U[k][q], F[k][q]);
+        // k = 3, 4: the pairs (2,3) and (1,4) with their lanes swapped
+        P[q][3] = make_float2(fmaf(1.5f, U[2][q].y, F[2][q].y), fmaf(-1.5f, U[2][q].x, F[2][q].x));
+        P[q][4] = make_float2(fmaf(1.5f, U[1][q].y, F[1][q].y), fmaf(-1.5f, U[1][q].x, F[1][q].x));
+    }
 }
 
 template <int DIR, bool CHAR, bool BORGES>

@@ -52,8 +52,18 @@ struct MarchTile {
     static constexpr int RING = 7;
     static constexpr int NFY = (TY + 1) * TZ, NFZ = TY * (TZ + 1);
     static constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
-    static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) + (size_t)5 * (NFY + NFZ) * sizeof(T);
+    // ring, y/z face buffers, and the FP64 conserved state of the plane in flight
+    static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) + (size_t)5 * (NFY + NFZ) * sizeof(T) +
+                                   (size_t)5 * NP * sizeof(double);
 };
+
+// 8-byte asynchronous global -> shared copies (cp.async, completion per thread)
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <typename T>
 __device__ __forceinline__ int ring_slot(int i, int x0) {
@@ -167,27 +177,42 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
     T* ring = reinterpret_cast<T*>(smem);  // [RING][5][NP]
     T* FY = ring + M::RING * 5 * M::NP;    // [5][NFY]
     T* FZ = FY + 5 * M::NFY;               // [5][NFZ]
+    double* S = reinterpret_cast<double*>(FZ + 5 * M::NFZ);  // [5][NP] U_in of the plane in flight
     const int tid = threadIdx.x, ty = tid / M::TZ, tz = tid % M::TZ;
     const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * M::LX;
     const int x1 = min(x0 + M::LX, b.nx);
     const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
     auto plane = [&](int i) { return ring + ring_slot<T>(i, x0) * 5 * M::NP; };
-    // W = prim(U_in) of plane i at folded positions
-    auto load_plane = [&](int i) {
-        T* P = plane(i);
+    // U_in of plane i at folded positions, into S without waiting (each thread
+    // later converts exactly the elements it copied, so S needs no barrier)
+    auto issue_plane = [&](int i) {
         const int gi = fold(i, b.nx, c.periodic[0]);
         for (int e = tid; e < M::NP; e += FT) {
             int py = e / M::PZ, pz = e % M::PZ;
             int gj = fold(j0 - 3 + py, b.ny, c.periodic[1]);
             int gk = fold(k0 - 3 + pz, b.nz, c.periodic[2]);
             long long o = b.at(gi + NG, gj + NG, gk + NG);
+#pragma unroll
+            for (int q = 0; q < 5; q++) cp_async8(S + q * M::NP + e, Uin + q * b.fstride + o);
+        }
+        cp_async_commit();
+    };
+    // W = prim(U_in) of the plane in S into plane i's ring slot
+    auto convert_plane = [&](int i) {
+        cp_async_wait_all();
+        T* P = plane(i);
+        for (int e = tid; e < M::NP; e += FT) {
             double u[5], w[5];
 #pragma unroll
-            for (int q = 0; q < 5; q++) u[q] = Uin[q * b.fstride + o];
+            for (int q = 0; q < 5; q++) u[q] = S[q * M::NP + e];
             prim_from_cons(u, c.gm1, w);
 #pragma unroll
             for (int q = 0; q < 5; q++) P[q * M::NP + e] = T(w[q]);
         }
+    };
+    auto load_plane = [&](int i) {
+        issue_plane(i);
+        convert_plane(i);
     };
     // x-face of this thread's column between cells i and i+1 (stencil i-2..i+3)
     const int ccol = (ty + 3) * M::PZ + (tz + 3);
@@ -198,6 +223,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
         march_face<0, CHAR, BORGES, T>(P, ccol, 0, M::NP, gamma, inv_gm1, out);
     };
     for (int i = x0 - 3; i < x0 + 3; i++) load_plane(i);
+    issue_plane(x0 + 3);
     __syncthreads();
     T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
     const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
@@ -212,8 +238,9 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
     const bool own = row && gj < b.ny && gk < b.nz;
     double best = INFINITY;
     for (int i = x0; i < x1; i++) {
-        load_plane(i + 3);
+        convert_plane(i + 3);
         __syncthreads();
+        if (i + 1 < x1) issue_plane(i + 4);  // in flight during this plane's faces and update
         const T* Pi = plane(i);
         if (conv_dims > 0) {
             if (row) xface(i, fxr);
