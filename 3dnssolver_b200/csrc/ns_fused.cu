@@ -45,16 +45,24 @@ constexpr int FT = 256;  // threads per block
 #ifndef NS_MARCH_TY
 #define NS_MARCH_TY 8
 #endif
-template <typename T>
+//
+// Plane i reads planes i-2..i+3 (x-faces) and i-H..i+H (viscous terms).  With
+// H <= 1 ("lean") the ring holds 6 planes and the y/z face buffers alternate
+// between planes, so a plane needs two block barriers instead of three: the
+// next plane's conversion overwrites plane i-2, whose last reader (the x-faces)
+// finished before this plane's second barrier.
+template <typename T, int H = 1>
 struct MarchTile {
     static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = 32;
     static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
-    static constexpr int RING = 7;
+    static constexpr bool LEAN = H <= 1;
+    static constexpr int RING = LEAN ? 6 : 7;
+    static constexpr int NBUF = LEAN ? 2 : 1;
     static constexpr int NFY = (TY + 1) * TZ, NFZ = TY * (TZ + 1);
     static constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
     // ring, y/z face buffers, and the FP64 conserved state of the plane in flight
-    static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) + (size_t)5 * (NFY + NFZ) * sizeof(T) +
-                                   (size_t)5 * NP * sizeof(double);
+    static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) +
+                                   (size_t)NBUF * 5 * (NFY + NFZ) * sizeof(T) + (size_t)5 * NP * sizeof(double);
 };
 
 // 8-byte asynchronous global -> shared copies (cp.async, completion per thread)
@@ -65,9 +73,9 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <typename T>
+template <int RING>
 __device__ __forceinline__ int ring_slot(int i, int x0) {
-    return (i - x0 + 3) % MarchTile<T>::RING;  // i >= x0 - 3
+    return (i - x0 + 3) % RING;  // i >= x0 - 3
 }
 
 // one face from a 6-cell stencil in a shared array with stride `step`
@@ -167,22 +175,22 @@ __device__ __forceinline__ void march_viscous(PlaneFn plane, int i, int cc, cons
 }
 
 template <typename T, bool CHAR, bool BORGES, int H, bool LAST>
-__global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
+__global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     k_stage_march(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
                   Consts c, int conv_dims, double m1, double m2, double mc,
                   const unsigned long long* __restrict__ slot, unsigned long long* slot_next,
                   double* clock) {
-    using M = MarchTile<T>;
+    using M = MarchTile<T, H>;
     extern __shared__ __align__(16) unsigned char smem[];
-    T* ring = reinterpret_cast<T*>(smem);  // [RING][5][NP]
-    T* FY = ring + M::RING * 5 * M::NP;    // [5][NFY]
-    T* FZ = FY + 5 * M::NFY;               // [5][NFZ]
-    double* S = reinterpret_cast<double*>(FZ + 5 * M::NFZ);  // [5][NP] U_in of the plane in flight
+    T* ring = reinterpret_cast<T*>(smem);        // [RING][5][NP]
+    T* FYb = ring + M::RING * 5 * M::NP;         // [NBUF][5][NFY]
+    T* FZb = FYb + M::NBUF * 5 * M::NFY;         // [NBUF][5][NFZ]
+    double* S = reinterpret_cast<double*>(FZb + M::NBUF * 5 * M::NFZ);  // [5][NP] U_in of the plane in flight
     const int tid = threadIdx.x, ty = tid / M::TZ, tz = tid % M::TZ;
     const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * M::LX;
     const int x1 = min(x0 + M::LX, b.nx);
     const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
-    auto plane = [&](int i) { return ring + ring_slot<T>(i, x0) * 5 * M::NP; };
+    auto plane = [&](int i) { return ring + ring_slot<M::RING>(i, x0) * 5 * M::NP; };
     // U_in of plane i at folded positions, into S without waiting (each thread
     // later converts exactly the elements it copied, so S needs no barrier)
     auto issue_plane = [&](int i) {
@@ -228,6 +236,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
     T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
     const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
     if (conv_dims > 0 && row) xface(x0 - 1, fxl);
+    if constexpr (M::LEAN) __syncthreads();  // plane x0+3 takes the slot of plane x0-3
     const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
     const double m3 = mc * dt;
     if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) {
@@ -242,6 +251,8 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
         __syncthreads();
         if (i + 1 < x1) issue_plane(i + 4);  // in flight during this plane's faces and update
         const T* Pi = plane(i);
+        T* FY = FYb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFY;
+        T* FZ = FZb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFZ;
         if (conv_dims > 0) {
             if (row) xface(i, fxr);
             // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
@@ -266,6 +277,13 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
         }
         __syncthreads();
         if (own) {
+            const long long o = b.at(i + NG, gj + NG, gk + NG);
+            double u0[5], ui[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) {  // issued before the viscous terms hide their latency
+                u0[q] = U0[q * b.fstride + o];
+                ui[q] = Uin[q * b.fstride + o];
+            }
             double r[5] = {0, 0, 0, 0, 0};
             if (conv_dims > 0) {
 #pragma unroll
@@ -284,34 +302,32 @@ __global__ void __launch_bounds__(FT, MarchTile<T>::MINB)
 #pragma unroll
                 for (int q = 1; q < 5; q++) r[q] += double(rv[q]);
             }
-            long long o = b.at(i + NG, gj + NG, gk + NG);
             double un[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) {
-                long long a = q * b.fstride + o;
-                un[q] = (U0[a] * m1) + (Uin[a] * m2) + (r[q] * m3);
-                Uout[a] = un[q];
+                un[q] = (u0[q] * m1) + (ui[q] * m2) + (r[q] * m3);
+                Uout[q * b.fstride + o] = un[q];
             }
             if constexpr (LAST) {
-                double w[5], u0[5];
+                double w[5], un0[5];
                 prim_from_cons(un, c.gm1, w);
                 double d = local_dt(w, c);
                 if (d < best) best = d;
-                cons_from_prim(w, c.inv_gm1, u0);
+                cons_from_prim(w, c.inv_gm1, un0);
 #pragma unroll
-                for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u0[q];
+                for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = un0[q];
             }
         }
 #pragma unroll
         for (int q = 0; q < 5; q++) fxl[q] = fxr[q];
-        __syncthreads();
+        if constexpr (!M::LEAN) __syncthreads();
     }
     if constexpr (LAST) block_min_to(best, slot_next);
 }
 
 template <typename T, bool CHAR, bool BORGES, int H, bool LAST>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
-    using M = MarchTile<T>;
+    using M = MarchTile<T, H>;
     auto kern = k_stage_march<T, CHAR, BORGES, H, LAST>;
     // the attribute is per device; setting it on every launch keeps multi-device use correct
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
