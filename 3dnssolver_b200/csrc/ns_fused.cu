@@ -73,6 +73,12 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Thread index rotated so that warp w handles items 0..31 of every round of a
+// pass: the partial last round of each pass (plane loads, y-faces, z-faces)
+// then falls to a different warp instead of piling up on warp 0 before the
+// same barrier.
+__device__ __forceinline__ int rotated(int tid, int w) { return (tid + FT - 32 * w) % FT; }
+
 template <int RING>
 __device__ __forceinline__ int ring_slot(int i, int x0) {
     return (i - x0 + 3) % RING;  // i >= x0 - 3
@@ -195,7 +201,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     // later converts exactly the elements it copied, so S needs no barrier)
     auto issue_plane = [&](int i) {
         const int gi = fold(i, b.nx, c.periodic[0]);
-        for (int e = tid; e < M::NP; e += FT) {
+        for (int e = rotated(tid, 5); e < M::NP; e += FT) {
             int py = e / M::PZ, pz = e % M::PZ;
             int gj = fold(j0 - 3 + py, b.ny, c.periodic[1]);
             int gk = fold(k0 - 3 + pz, b.nz, c.periodic[2]);
@@ -209,7 +215,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     auto convert_plane = [&](int i) {
         cp_async_wait_all();
         T* P = plane(i);
-        for (int e = tid; e < M::NP; e += FT) {
+        for (int e = rotated(tid, 5); e < M::NP; e += FT) {
             double u[5], w[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) u[q] = S[q * M::NP + e];
@@ -256,7 +262,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
         if (conv_dims > 0) {
             if (row) xface(i, fxr);
             // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
-            for (int e = tid; e < M::NFY; e += FT) {
+            for (int e = rotated(tid, 7); e < M::NFY; e += FT) {
                 int fb = e / M::TZ, cz = e % M::TZ;
                 const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                 T out[5];
@@ -265,7 +271,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
                 for (int q = 0; q < 5; q++) FY[q * M::NFY + e] = out[q];
             }
             if (conv_dims == 3) {
-                for (int e = tid; e < M::NFZ; e += FT) {
+                for (int e = rotated(tid, 6); e < M::NFZ; e += FT) {
                     int ry = e / (M::TZ + 1), fc = e % (M::TZ + 1);
                     const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                     T out[5];
