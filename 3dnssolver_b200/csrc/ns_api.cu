@@ -113,6 +113,8 @@ static ns_status validate(const ns_params* p) {
             return fail(NS_ERR_INVALID_ARG, "the sensor gates the characteristic scheme: convection must be NS_CONV_WENO5_CHAR");
         if (p->precision != NS_PREC_FP32)
             return fail(NS_ERR_INVALID_ARG, "the sensor-gated form runs in NS_PREC_FP32");
+        if (p->semantics != NS_SEM_REFERENCE)
+            return fail(NS_ERR_INVALID_ARG, "the sensor-gated form follows the reference semantics");
         if (!(p->sensor_threshold > 0.0 && p->sensor_threshold < 1.0))
             return fail(NS_ERR_INVALID_ARG, "sensor_threshold must lie in (0,1)");
     }
@@ -289,6 +291,19 @@ static ns_status do_step_fused(ns_ctx* ctx) {
     a.U0 = ctx->U0;
     a.slot = cur;
     a.slot_next = nxt;
+    if (p.sensor && a.conv_dims > 0) {
+        // the network on the step's start state; its flags gate the three stages
+        for (int d = 0; d < a.conv_dims; d++) {
+            if (sensor_step_mask(ctx->sensor, d, ctx->U0, ctx->box, ctx->c, p.sensor_threshold, ctx->fb[d], s,
+                                 &ctx->launches) != NS_OK)
+                return fail(NS_ERR_CUDA, "sensor flag kernel launch failed: %s",
+                            cudaGetErrorString(cudaGetLastError()));
+            a.gate.m[d] = sensor_mask(ctx->sensor, d);
+            a.gate.fb[d] = ctx->fb[d];
+        }
+        a.gated = true;
+        prof_mark(ctx, NS_PROF_SENSOR);
+    }
     // SSP-RK3 coefficients (time_scheme.cpp:36-38, 48-50, 60-62); U0 -> U -> U2 -> U
     const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
     const double m2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
@@ -481,7 +496,7 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
     // overlap the load and compute phases with, and the FP64-pipe-bound face
     // kernels of the unfused path run faster (measured on B200 at 256^3:
     // 2.18 vs 3.06 G cell-updates/s for the characteristic scheme).
-    ctx->fused = (p->semantics == NS_SEM_REFERENCE) && !p->sensor && p->precision == NS_PREC_FP32;
+    ctx->fused = (p->semantics == NS_SEM_REFERENCE) && p->precision == NS_PREC_FP32;
     if (ctx->fused) A((void**)&ctx->U2, soa_bytes(ctx->box));
     A((void**)&ctx->diag, 8 * sizeof(double));
     A((void**)&ctx->clock, 2 * sizeof(double));
@@ -683,7 +698,7 @@ ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out) {
 }
 
 ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
-    if (!ctx || !ms || n < NS_PROF_N) return fail(NS_ERR_INVALID_ARG, "ctx/ms invalid or n < NS_PROF_N");
+    if (!ctx || !ms || n < 7) return fail(NS_ERR_INVALID_ARG, "ctx/ms invalid or n < 7");
     if (!ctx->w_valid && !ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no state has been uploaded");
     Prof pr;
     for (int e = 0; e < 64; e++) NS_CUDA(cudaEventCreate(&pr.ev[e]));
@@ -700,7 +715,7 @@ ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
     for (int e = 0; e < pr.n && st == NS_OK; e++) {
         float t = 0.f;
         cudaEventElapsedTime(&t, prev, pr.ev[e]);
-        ms[pr.cls[e]] += t;
+        if (pr.cls[e] < n) ms[pr.cls[e]] += t;
         prev = pr.ev[e];
     }
     for (int e = 0; e < 64; e++) cudaEventDestroy(pr.ev[e]);

@@ -85,11 +85,19 @@ __device__ __forceinline__ int ring_slot(int i, int x0) {
 }
 
 // one face from a 6-cell stencil in a shared array with stride `step`
-template <int DIR, bool CHAR, bool BORGES, typename T>
+// (GATE: the characteristic-wise form where `fire`, the component-wise elsewhere)
+template <int DIR, bool CHAR, bool BORGES, bool GATE, typename T>
 __device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, T gamma,
-                                           T inv_gm1, T out[5]) {
+                                           T inv_gm1, bool fire, T out[5]) {
     if constexpr (sizeof(T) == 4) {
-        face_f32x2<DIR, CHAR, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
+        if constexpr (GATE) {
+            if (fire)
+                face_f32x2<DIR, true, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
+            else
+                face_f32x2<DIR, false, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
+        } else {
+            face_f32x2<DIR, CHAR, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
+        }
         return;
     }
     const T hg = T(0.5) * gamma * inv_gm1;
@@ -180,13 +188,14 @@ __device__ __forceinline__ void march_viscous(PlaneFn plane, int i, int cc, cons
                                P[H][1 * fs + cc], P[H][cc], c, r);
 }
 
-template <typename T, bool CHAR, bool BORGES, int H, bool LAST>
+template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool GATE>
 __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     k_stage_march(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
                   Consts c, int conv_dims, double m1, double m2, double mc,
                   const unsigned long long* __restrict__ slot, unsigned long long* slot_next,
-                  double* clock) {
+                  double* clock, Gate gate) {
     using M = MarchTile<T, H>;
+    static_assert(M::NFY <= 2 * FT && M::NFZ <= 2 * FT, "a face pass takes at most two rounds");
     extern __shared__ __align__(16) unsigned char smem[];
     T* ring = reinterpret_cast<T*>(smem);        // [RING][5][NP]
     T* FYb = ring + M::RING * 5 * M::NP;         // [NBUF][5][NFY]
@@ -230,18 +239,41 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     };
     // x-face of this thread's column between cells i and i+1 (stencil i-2..i+3)
     const int ccol = (ty + 3) * M::PZ + (tz + 3);
-    auto xface = [&](int i, T out[5]) {
+    auto xface = [&](int i, bool fire, T out[5]) {
         const T* P[6];
 #pragma unroll
         for (int s = 0; s < 6; s++) P[s] = plane(i - 2 + s);
-        march_face<0, CHAR, BORGES, T>(P, ccol, 0, M::NP, gamma, inv_gm1, out);
+        march_face<0, CHAR, BORGES, GATE, T>(P, ccol, 0, M::NP, gamma, inv_gm1, fire, out);
+    };
+    const int gj = j0 + ty, gk = k0 + tz;
+    const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
+    const bool own = row && gj < b.ny && gk < b.nz;
+    // sensor flags of this thread's faces of plane i (x-face i+1/2, up to two y- and
+    // two z-faces), loaded early and tested only in the face pass; i = x0 - 1 (the
+    // first x-face) can be -1, which has no y- or z-faces
+    unsigned char gx = 0, gy[2] = {0, 0}, gz[2] = {0, 0};
+    auto load_flags = [&](int i) {
+        if constexpr (GATE) {
+            gx = own ? gate.m[0][gate.fb[0].at(i + 1, gj, gk)] : 0;
+#pragma unroll
+            for (int r = 0; r < 2; r++) {
+                int e = rotated(tid, 7) + r * FT;
+                int a = j0 + e / M::TZ, kk = k0 + e % M::TZ;
+                gy[r] = (i >= 0 && e < M::NFY && a <= b.ny && kk < b.nz) ? gate.m[1][gate.fb[1].at(i, a, kk)] : 0;
+                e = rotated(tid, 6) + r * FT;
+                int jj = j0 + e / (M::TZ + 1);
+                a = k0 + e % (M::TZ + 1);
+                gz[r] = (i >= 0 && conv_dims == 3 && e < M::NFZ && jj < b.ny && a <= b.nz)
+                            ? gate.m[2][gate.fb[2].at(i, jj, a)] : 0;
+            }
+        }
     };
     for (int i = x0 - 3; i < x0 + 3; i++) load_plane(i);
     issue_plane(x0 + 3);
     __syncthreads();
     T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
-    const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
-    if (conv_dims > 0 && row) xface(x0 - 1, fxl);
+    load_flags(x0 - 1);
+    if (conv_dims > 0 && row) xface(x0 - 1, gx != 0, fxl);
     if constexpr (M::LEAN) __syncthreads();  // plane x0+3 takes the slot of plane x0-3
     const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
     const double m3 = mc * dt;
@@ -249,33 +281,37 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
         clock[0] = dt;
         clock[1] += dt;
     }
-    const int gj = j0 + ty, gk = k0 + tz;
-    const bool own = row && gj < b.ny && gk < b.nz;
     double best = INFINITY;
     for (int i = x0; i < x1; i++) {
+        load_flags(i);
         convert_plane(i + 3);
         __syncthreads();
         if (i + 1 < x1) issue_plane(i + 4);  // in flight during this plane's faces and update
         const T* Pi = plane(i);
         T* FY = FYb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFY;
         T* FZ = FZb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFZ;
+        // GATE: a flagged face takes the characteristic-wise branch in its own lane
+        // (a dense recompute of the block's flagged faces after the pass measured
+        // slower: it adds a block-wide round and a barrier to every plane)
         if (conv_dims > 0) {
-            if (row) xface(i, fxr);
+            if (row) xface(i, gx != 0, fxr);
             // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
-            for (int e = rotated(tid, 7); e < M::NFY; e += FT) {
+            for (int e = rotated(tid, 7), r = 0; e < M::NFY; e += FT, r++) {
                 int fb = e / M::TZ, cz = e % M::TZ;
                 const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                 T out[5];
-                march_face<1, CHAR, BORGES, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1, out);
+                march_face<1, CHAR, BORGES, GATE, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1,
+                                                     gy[r] != 0, out);
 #pragma unroll
                 for (int q = 0; q < 5; q++) FY[q * M::NFY + e] = out[q];
             }
             if (conv_dims == 3) {
-                for (int e = rotated(tid, 6); e < M::NFZ; e += FT) {
+                for (int e = rotated(tid, 6), r = 0; e < M::NFZ; e += FT, r++) {
                     int ry = e / (M::TZ + 1), fc = e % (M::TZ + 1);
                     const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                     T out[5];
-                    march_face<2, CHAR, BORGES, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1, out);
+                    march_face<2, CHAR, BORGES, GATE, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1,
+                                                         gz[r] != 0, out);
 #pragma unroll
                     for (int q = 0; q < 5; q++) FZ[q * M::NFZ + e] = out[q];
                 }
@@ -331,31 +367,41 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     if constexpr (LAST) block_min_to(best, slot_next);
 }
 
-template <typename T, bool CHAR, bool BORGES, int H, bool LAST>
+template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool GATE>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
     using M = MarchTile<T, H>;
-    auto kern = k_stage_march<T, CHAR, BORGES, H, LAST>;
+    auto kern = k_stage_march<T, CHAR, BORGES, H, LAST, GATE>;
     // the attribute is per device; setting it on every launch keeps multi-device use correct
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
     if (e != cudaSuccess) return e;
     dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + M::LX - 1) / M::LX);
     kern<<<grid, FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
-                                   a.slot_next, a.clock);
+                                   a.slot_next, a.clock, a.gate);
     return cudaGetLastError();
 }
 
-template <typename T, bool CHAR, bool BORGES, bool LAST>
+template <typename T, bool CHAR, bool BORGES, bool LAST, bool GATE = false>
 static cudaError_t fused_h(const FusedArgs& a, cudaStream_t s) {
     switch (a.visc_h) {
-        case 0: return fused_one<T, CHAR, BORGES, 0, LAST>(a, s);
-        case 1: return fused_one<T, CHAR, BORGES, 1, LAST>(a, s);
-        case 2: return fused_one<T, CHAR, BORGES, 2, LAST>(a, s);
-        default: return fused_one<T, CHAR, BORGES, 3, LAST>(a, s);
+        case 0: return fused_one<T, CHAR, BORGES, 0, LAST, GATE>(a, s);
+        case 1: return fused_one<T, CHAR, BORGES, 1, LAST, GATE>(a, s);
+        case 2: return fused_one<T, CHAR, BORGES, 2, LAST, GATE>(a, s);
+        default: return fused_one<T, CHAR, BORGES, 3, LAST, GATE>(a, s);
     }
 }
 
 template <typename T>
 static cudaError_t fused_t(const FusedArgs& a, cudaStream_t s) {
+    if (a.gated) {  // learned-sensor gate: FP32 characteristic-wise form only
+        if constexpr (sizeof(T) == 8) {
+            return cudaErrorInvalidValue;
+        } else {
+            if (!a.chr) return cudaErrorInvalidValue;
+            if (a.borges)
+                return a.last ? fused_h<T, true, true, true, true>(a, s) : fused_h<T, true, true, false, true>(a, s);
+            return a.last ? fused_h<T, true, false, true, true>(a, s) : fused_h<T, true, false, false, true>(a, s);
+        }
+    }
     if (a.chr) {
         if (a.borges) return a.last ? fused_h<T, true, true, true>(a, s) : fused_h<T, true, true, false>(a, s);
         return a.last ? fused_h<T, true, false, true>(a, s) : fused_h<T, true, false, false>(a, s);

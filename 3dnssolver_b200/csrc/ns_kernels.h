@@ -29,6 +29,12 @@ struct UpdateArgs {
     double* clock;                   // [last dt, accumulated time], updated once per step (nullable)
 };
 
+// per-face flags of the learned sensor (1 = characteristic-wise), FaceBox order
+struct Gate {
+    const unsigned char* m[3];
+    FaceBox fb[3];
+};
+
 // one fused SSP-RK3 stage (ns_fused.cu)
 struct FusedArgs {
     const double* Uin;
@@ -43,6 +49,8 @@ struct FusedArgs {
     const unsigned long long* slot;   // CFL minimum of this step
     unsigned long long* slot_next;    // last stage: CFL minimum of the next step
     double* clock;                    // first stage: [last dt, accumulated time]
+    bool gated;                       // characteristic-wise only where gate flags a face (FP32)
+    Gate gate;
 };
 cudaError_t launch_stage_fused(const FusedArgs& a, cudaStream_t s);
 

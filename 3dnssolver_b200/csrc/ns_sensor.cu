@@ -25,6 +25,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -34,6 +35,7 @@
 #include <vector>
 
 #include "ns_common.cuh"
+#include "ns_eos.cuh"
 #include "ns_face.cuh"
 #include "ns_sensor.h"
 
@@ -594,24 +596,100 @@ __global__ void __launch_bounds__(128) k_face_gated(const double* __restrict__ W
 }
 
 // ---------------------------------------------------------------------------
+// per-step flags for the fused stage kernel: the MLP on every face along DIR of
+// the step's start state U0 (W = prim(U0) at boundary-folded cells, the
+// stage kernel's own halo rule), one byte per face (1 = characteristic-wise)
+
+template <int DIR>
+__global__ void __launch_bounds__(128) k_sensor_mask(const double* __restrict__ U0, Box b, Consts c,
+                                                     FaceBox fb, const float* __restrict__ w,
+                                                     float logit_thr, unsigned char* __restrict__ mask,
+                                                     unsigned long long* __restrict__ flagged) {
+    __shared__ __align__(16) MlpSmem m;
+    __shared__ __align__(16) __nv_bfloat16 Xs[4][32 * XS];
+    const int warp = threadIdx.y, lane = threadIdx.x;
+    mlp_load(m, w, false);  // once per block: the grid strides over 32 x 4 tiles of faces
+    __syncthreads();
+    const float gm1 = float(c.gm1), gamma = float(c.gamma);
+    const int t2 = (fb.n2 + 31) / 32, t1 = (fb.n1 + 3) / 4;
+    const long long tiles = (long long)t2 * t1 * fb.n0;
+    __nv_bfloat16* X = Xs[warp];
+    unsigned long long nfire = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int kk = (int)(t % t2) * 32 + lane;
+        const int bb = (int)((t / t2) % t1) * 4 + warp;
+        const int aa = (int)(t / ((long long)t2 * t1));
+        const bool live = kk < fb.n2 && bb < fb.n1;
+        float feat[SF];
+        if (live) {
+            // face aa lies between cells aa-1 and aa along DIR: stencil aa-3..aa+2;
+            // rho, p and u_n in FP32 (the network reads BF16 features)
+            float rho[6], p[6], un[6];
+#pragma unroll
+            for (int s = 0; s < 6; s++) {
+                int i = aa, j = bb, k = kk;
+                if (DIR == 0) i = fold(aa - 3 + s, b.nx, c.periodic[0]);
+                if (DIR == 1) j = fold(bb - 3 + s, b.ny, c.periodic[1]);
+                if (DIR == 2) k = fold(kk - 3 + s, b.nz, c.periodic[2]);
+                const long long o = b.at(i + NG, j + NG, k + NG);
+                float u[5];
+#pragma unroll
+                for (int q = 0; q < 5; q++) u[q] = float(U0[q * b.fstride + o]);
+                const float ir = __fdividef(1.f, u[0]);
+                rho[s] = u[0];
+                un[s] = u[2 + DIR] * ir;
+                p[s] = gm1 * (u[1] - 0.5f * ir * (u[2] * u[2] + u[3] * u[3] + u[4] * u[4]));
+            }
+            face_features<float>(rho, p, un, gamma, feat);
+        } else {
+#pragma unroll
+            for (int e = 0; e < SF; e++) feat[e] = 0.f;
+        }
+        __syncwarp();  // the previous tile's fragments are read
+#pragma unroll
+        for (int e = 0; e < XS; e++) X[lane * XS + e] = __float2bfloat16(e < SF ? feat[e] : 0.f);
+        __syncwarp();
+        MlpFwd f;
+        mlp_forward(m, X, f);
+        float lg = 0.f;
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                float v = __shfl_sync(0xffffffffu, f.lg[mt][h], 4 * (lane & 7));
+                if ((lane >> 4) == mt && ((lane >> 3) & 1) == h) lg = v;
+            }
+        const bool fire = live && lg > logit_thr;
+        if (live) mask[fb.at(aa, bb, kk)] = fire ? 1 : 0;
+        nfire += __popc(__ballot_sync(0xffffffffu, fire));
+    }
+    if (lane == 0 && nfire) atomicAdd(flagged, nfire);
+}
+
+// ---------------------------------------------------------------------------
 // context-side state
 
 struct SensorState {
     float* w = nullptr;                    // FP32 parameters on the device
     unsigned long long* flagged = nullptr;  // faces flagged since creation
+    unsigned char* mask[3] = {nullptr, nullptr, nullptr};  // per-step flags, one byte per face
     unsigned long long faces = 0;           // faces evaluated since creation (host count)
+    int sms = 148;                          // multiprocessors of the context's device
     bool has_weights = false;
 };
 
-ns_status sensor_create(SensorState** out, const Box&, const FaceBox*, cudaStream_t s) {
+ns_status sensor_create(SensorState** out, const Box&, const FaceBox* fb, cudaStream_t s) {
     *out = nullptr;
     SensorState* st = new (std::nothrow) SensorState();
     if (!st) return NS_ERR_OOM;
-    if (cudaMalloc(&st->w, SP * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&st->flagged, sizeof(unsigned long long)) != cudaSuccess) {
-        cudaFree(st->w);
-        cudaFree(st->flagged);
-        delete st;
+    bool ok = cudaMalloc(&st->w, SP * sizeof(float)) == cudaSuccess &&
+              cudaMalloc(&st->flagged, sizeof(unsigned long long)) == cudaSuccess;
+    for (int d = 0; d < 3 && ok; d++) ok = cudaMalloc(&st->mask[d], (size_t)fb[d].fstride) == cudaSuccess;
+    int dev = 0;
+    if (ok && cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&st->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (!ok) {
+        sensor_destroy(st);
         cudaGetLastError();
         return NS_ERR_OOM;
     }
@@ -625,6 +703,7 @@ void sensor_destroy(SensorState* st) {
     if (!st) return;
     cudaFree(st->w);
     cudaFree(st->flagged);
+    for (int d = 0; d < 3; d++) cudaFree(st->mask[d]);
     delete st;
 }
 
@@ -656,6 +735,22 @@ ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const doub
     if (launches) (*launches)++;
     return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;
 }
+
+ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box& b, const Consts& c,
+                           double threshold, const FaceBox& fb, cudaStream_t s, long long* launches) {
+    const float thr = (float)std::log(threshold / (1.0 - threshold));
+    const long long tiles = (long long)((fb.n2 + 31) / 32) * ((fb.n1 + 3) / 4) * fb.n0;
+    const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
+    const dim3 blk(32, 4);
+    if (dir == 0) k_sensor_mask<0><<<grid, blk, 0, s>>>(U0, b, c, fb, st->w, thr, st->mask[0], st->flagged);
+    else if (dir == 1) k_sensor_mask<1><<<grid, blk, 0, s>>>(U0, b, c, fb, st->w, thr, st->mask[1], st->flagged);
+    else k_sensor_mask<2><<<grid, blk, 0, s>>>(U0, b, c, fb, st->w, thr, st->mask[2], st->flagged);
+    st->faces += (unsigned long long)fb.n0 * fb.n1 * fb.n2;
+    if (launches) (*launches)++;
+    return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;
+}
+
+const unsigned char* sensor_mask(const SensorState* st, int dir) { return st->mask[dir]; }
 
 double sensor_last_fraction(SensorState* st) {
     if (!st || st->faces == 0) return 0.0;

@@ -17,6 +17,11 @@ void sensor_destroy(SensorState* st);
 ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const double* U, const Box& b,
                            const Consts& c, double threshold, bool borges, void* F,
                            const FaceBox& fb, cudaStream_t s, long long* launches);
+// Per-step flags along axis dir for the fused stage kernel: the network on every
+// face of the step's start state U0, one byte per face (FaceBox order).
+ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box& b, const Consts& c,
+                           double threshold, const FaceBox& fb, cudaStream_t s, long long* launches);
+const unsigned char* sensor_mask(const SensorState* st, int dir);
 // fraction of evaluated faces the sensor flagged since the context was created
 double sensor_last_fraction(SensorState* st);
 ns_status sensor_set_weights(SensorState* st, const float* w, cudaStream_t s);

@@ -262,8 +262,11 @@ def rooflines(form, prof, n, peaks, fma):
     alg = {"face_x": face_bytes, "face_y": face_bytes, "face_z": face_bytes,
            "update": cells * (3 * 40) + 3 * faces * 5 * elem + cells * 40,
            "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120,
-           "stage_fused": cells * 120}
-    kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})"}.get(
+           "stage_fused": cells * 120,
+           # per-step sensor flags: U0 read once per axis, one byte per face written
+           "sensor": 3 * (cells * 40 + faces)}
+    kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})",
+             "sensor": f"k_sensor_mask ({form})"}.get(
         dom, f"k_face_flux ({dom}, {form})" if dom.startswith("face") else dom)
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
@@ -411,9 +414,14 @@ def main():
     # headline form's: relative L2 error per conserved field against it
     g3 = slice(3, -3)
     forms = {args.form: {"value": value, "ms_per_step": ms_max / args.steps}}
+    if FORMS[args.form][2]:
+        forms[args.form]["sensor_fraction"] = diag["sensor_fraction"]
+        forms[args.form]["sensor_training"] = sensor_info
     U_ref = None
     if args.also:
         s0 = pkg.Solver(p)
+        if FORMS[args.form][2]:
+            s0.set_sensor_weights(sensor_w)
         s0.upload_primitive(W0)
         s0.advance(args.warmup + args.steps)
         U_ref = s0.download_conservative()[g3, g3, g3]

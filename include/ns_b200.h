@@ -157,19 +157,25 @@ NS_API ns_status ns_advance(ns_ctx* ctx, int nsteps);
  * check_finite was requested and the state holds NaN/Inf. */
 NS_API ns_status ns_synchronize(ns_ctx* ctx);
 NS_API ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
-/* Kernel classes timed by ns_profile_step */
+/* Kernel classes timed by ns_profile_step (NS_PROF_SENSOR: the per-step
+ * sensor flags of the fused FP32 form) */
 enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FACE_Y = 3,
-       NS_PROF_FACE_Z = 4, NS_PROF_UPDATE = 5, NS_PROF_STAGE_FUSED = 6, NS_PROF_N = 7 };
+       NS_PROF_FACE_Z = 4, NS_PROF_UPDATE = 5, NS_PROF_STAGE_FUSED = 6, NS_PROF_SENSOR = 7,
+       NS_PROF_N = 8 };
 /* Runs one time step of the device-resident state with CUDA events recorded
  * between its kernels on the context's stream; ms[c] receives the device time
- * of kernel class c summed over the step (n >= NS_PROF_N). */
+ * of kernel class c summed over the step, for c < n (n >= 7; classes at or
+ * above n are left out of ms). */
 NS_API ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n);
 /* ---- learned troubled-face sensor (no reference counterpart) ----------------
  * An MLP 21 -> 32 -> 32 -> 1 (GELU) predicts from a face's stencil whether the
  * characteristic-wise WENO-5 flux differs from the component-wise one by more
  * than a relative threshold; with ns_params.sensor = 1 (FP32 characteristic
- * form) the component-wise flux is used on every face and the characteristic
- * one is recomputed on the faces the network flags.  Parameters are
+ * form, reference semantics) the characteristic-wise flux is computed only on
+ * the faces the network flags and the component-wise flux elsewhere.  Time
+ * steps evaluate the network once per step, on the state at the step's start,
+ * and its flags gate all three stages; the per-operator entry points
+ * (ns_convection_solve, ns_rhs) evaluate it on the W they are given.  Parameters are
  * NS_SENSOR_NPARAMS floats: W1[32][32] (out, in; in >= 21 unused), b1[32],
  * W2[32][32], b2[32], w3[32], b3.  Device pointers below are caller-owned. */
 #define NS_SENSOR_FEATURES 21
