@@ -214,11 +214,11 @@ def job_rate(world, cells, steps, ms_max):
 # rooflines of the dominant kernel
 
 # Floating-point work per unit of each kernel class, counted by ncu on the 128^3
-# shear layer (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}_pred_on.sum
+# shear layer (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}[2]_pred_on.sum
 # divided by the faces or cells of the launch; the counts do not depend on the data):
-# (flop per unit with an FMA as 2, FP instructions per unit, pipe, unit).
-# The fused stage rows are the first two stages; the third adds the next step's
-# start (about 70 FP64 instructions per cell).
+# (flop per unit with an FMA as 2, FP lane operations per unit with a packed f32x2
+# operation as 2, pipe, unit).  The fused stage rows are the first two stages; the
+# third adds the next step's start (about 70 FP64 instructions per cell).
 COMPUTE_PER_UNIT = {
     ("fp64_char", "face_x"): (1325, 953, "fp64", "face"),
     ("fp64_char", "face_y"): (1325, 953, "fp64", "face"),
@@ -228,8 +228,8 @@ COMPUTE_PER_UNIT = {
     ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
     ("fp64_char", "update"): (316, 205, "fp64", "cell"),
     ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
-    ("fp32_char", "stage_fused"): (4112, 2928, "fp32", "cell"),
-    ("fp32_comp", "stage_fused"): (3022, 2279, "fp32", "cell"),
+    ("fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
+    ("fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
 }
 # DRAM bytes (read + write) per unit from the same capture; these kernels stream
 # their inputs once at 128^3 and above, so the traffic scales with the units.
@@ -285,14 +285,14 @@ def rooflines(form, prof, n, peaks, fma):
         flop_u, inst_u, pipe, unit = row
         peak = fma[pipe]
         tflops = flop_u * units / (per_launch_ms / 1000.0) / 1e12
-        # FP instructions against the FMA issue rate (peak / 2 flops): a multiply or add
+        # FP lane operations against the FMA rate (peak / 2 flops): a multiply or add
         # takes the same pipe slot as an FMA, so this is the pipe's busy fraction
-        inst_rate = inst_u * units / (per_launch_ms / 1000.0) / 1e12
+        ops_rate = inst_u * units / (per_launch_ms / 1000.0) / 1e12
         comp = {"bound": pipe, "kernel": kname, "achieved": round(tflops, 2), "peak": round(peak, 2),
                 "unit": "TFLOP/s", "frac": round(tflops / peak, 4),
-                "pipe_frac": round(inst_rate / (peak / 2.0), 4),
+                "pipe_frac": round(ops_rate / (peak / 2.0), 4),
                 "peak_source": f"measured now: ns_fma_peak ({pipe} FMA chains on every SM)",
-                "flop_per_" + unit: flop_u, "fp_inst_per_" + unit: inst_u}
+                "flop_per_" + unit: flop_u, "fp_ops_per_" + unit: inst_u}
         hbm["note"] = f"{pipe}-pipe bound: see compute_roofline"
     return hbm, comp
 
