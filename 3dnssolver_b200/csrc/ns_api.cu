@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <utility>
 #include <mutex>
 #include <new>
 #include <string>
@@ -57,7 +58,8 @@ struct ns_ctx {
     double* W = nullptr;   // primitive, halo'd SoA
     double* U = nullptr;   // conservative, halo'd SoA
     double* U0 = nullptr;  // RK stage base (interior used)
-    double* U2 = nullptr;  // second stage buffer of the fused path
+    double* U2 = nullptr;  // second stage buffer of the fused paths
+    bool xfused = false;   // FP64 steps: x-faces and update in one kernel (k_xface_update)
     double* R = nullptr;   // residual for the operator entry points (lazy)
     void* F[3] = {nullptr, nullptr, nullptr};
     double* stage = nullptr;              // host-layout staging (lazy)
@@ -219,12 +221,12 @@ static void prof_mark(ns_ctx* ctx, int cls) {
     g_prof->cls[g_prof->n++] = cls;
 }
 
-// face fluxes of the current (W, U) along every convected axis
-static ns_status faces(ns_ctx* ctx) {
+// face fluxes of the current (W, U) along every convected axis from first_dir on
+static ns_status faces(ns_ctx* ctx, int first_dir = 0) {
     const ns_params& p = ctx->p;
     if (p.convection == NS_CONV_NONE) return NS_OK;
     int nd = p.dim == 3 ? 3 : 2;
-    for (int d = 0; d < nd; d++) {
+    for (int d = first_dir; d < nd; d++) {
         if (p.sensor) {
             if (sensor_face_flux(ctx->sensor, d, ctx->W, ctx->U, ctx->box, ctx->c, p.sensor_threshold,
                                  p.weights == NS_WEIGHTS_BORGES, ctx->F[d], ctx->fb[d], ctx->stream,
@@ -345,20 +347,33 @@ static ns_status do_step(ns_ctx* ctx) {
     const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
     const double m2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
     const double mc[3] = {-1.0, -(1. / 4.), -(2. / 3.)};
+    // FP64 with convection: y- and z-faces, then the x-faces marched together with
+    // the cell update into the second state buffer (the buffers swap each stage;
+    // the fill copies the stage input's face halos into the output buffer, so the
+    // state ends every stage, and the step, with the halos the reference holds)
+    const bool xfused = ctx->xfused;
     for (int st = 0; st < 3; st++) {
-        launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
+        launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s, xfused ? ctx->U2 : nullptr);
         NS_TRY(check_launch(ctx, 1));
         prof_mark(ctx, NS_PROF_FILL);
-        NS_TRY(faces(ctx));
+        NS_TRY(faces(ctx, xfused ? 1 : 0));
         UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
         a.slot = cur;
         a.m1 = m1[st];
         a.m2 = m2[st];
         a.mc = mc[st];
         a.clock = (st == 0) ? ctx->clock : nullptr;
-        launch_update(a, s);
-        NS_TRY(check_launch(ctx, 1));
-        prof_mark(ctx, NS_PROF_UPDATE);
+        if (xfused) {
+            a.Unext = ctx->U2;
+            launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
+            NS_TRY(check_launch(ctx, 1));
+            std::swap(ctx->U, ctx->U2);
+            prof_mark(ctx, NS_PROF_XFACE_UPDATE);
+        } else {
+            launch_update(a, s);
+            NS_TRY(check_launch(ctx, 1));
+            prof_mark(ctx, NS_PROF_UPDATE);
+        }
     }
     ctx->u_valid = true;
     ctx->w_valid = false;
@@ -497,7 +512,8 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
     // kernels of the unfused path run faster (measured on B200 at 256^3:
     // 2.18 vs 3.06 G cell-updates/s for the characteristic scheme).
     ctx->fused = (p->semantics == NS_SEM_REFERENCE) && p->precision == NS_PREC_FP32;
-    if (ctx->fused) A((void**)&ctx->U2, soa_bytes(ctx->box));
+    ctx->xfused = !ctx->fused && p->precision == NS_PREC_FP64 && p->convection != NS_CONV_NONE;
+    if (ctx->fused || ctx->xfused) A((void**)&ctx->U2, soa_bytes(ctx->box));
     A((void**)&ctx->diag, 8 * sizeof(double));
     A((void**)&ctx->clock, 2 * sizeof(double));
     if (st == NS_OK) {

@@ -74,6 +74,16 @@ struct Consts {
     double df[7], ddf[7];       // CD coefficients, centred at index 3
 };
 
+#ifdef __CUDACC__
+// 8-byte asynchronous global -> shared copies (cp.async, completion per thread)
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+#endif
+
 // Periodic wrap or Neumann clamp of an interior-coordinate index.
 NS_HOST_DEVICE int fold(int i, int n, int periodic) {
     if (i >= 0 && i < n) return i;

@@ -65,13 +65,6 @@ struct MarchTile {
                                    (size_t)NBUF * 5 * (NFY + NFZ) * sizeof(T) + (size_t)5 * NP * sizeof(double);
 };
 
-// 8-byte asynchronous global -> shared copies (cp.async, completion per thread)
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-    unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Thread index rotated so that warp w handles items 0..31 of every round of a
 // pass: the partial last round of each pass (plane loads, y-faces, z-faces)

@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(128) k_min_dt(const double* __restrict__ W, Bo
 // then W = prim(U) on every cell (eq_of_state.cpp:61-87).
 
 __global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, double* __restrict__ U,
-                                                   Box b, Consts c) {
+                                                   Box b, Consts c, double* __restrict__ Uhalo) {
     int kh = blockIdx.x * 32 + threadIdx.x;
     int jh = blockIdx.y * 4 + threadIdx.y;
     int ih = blockIdx.z;
@@ -141,10 +141,15 @@ __global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, doubl
         for (int q = 0; q < 5; q++) {
             u[q] = U[q * b.fstride + s];
             U[q * b.fstride + o] = u[q];
+            if (Uhalo) Uhalo[q * b.fstride + o] = u[q];  // the stage's output buffer keeps the same halos
         }
     } else {
 #pragma unroll
         for (int q = 0; q < 5; q++) u[q] = U[q * b.fstride + o];
+        if (Uhalo && (ox || oy || oz)) {  // edges and corners travel unchanged as well
+#pragma unroll
+            for (int q = 0; q < 5; q++) Uhalo[q * b.fstride + o] = u[q];
+        }
     }
     prim_from_cons(u, c.gm1, w);
 #pragma unroll
@@ -424,6 +429,98 @@ __global__ void __launch_bounds__(128, NS_UPDATE_MINB) k_update(const double* __
 }
 
 // ---------------------------------------------------------------------------
+// FP64 stage, last kernel: x-face fluxes marched along x with the cell update of
+// each cell as soon as both of its x-faces are known (same face and update
+// arithmetic as k_face_flux<0> + k_update).  The x-face array never reaches
+// HBM, and the update's loads (U0, U, the y- and z-face fluxes, W for the
+// viscous terms) overlap the x-faces' FP64 work.  U_out is a second buffer:
+// other threads still read U's x-neighbours for their stencils.
+
+#ifndef NS_XMARCH_L
+#define NS_XMARCH_L 32
+#endif
+template <bool CHAR, bool BORGES, bool PHYS, int H>
+__global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
+    k_xface_update(const double* __restrict__ W, const double* __restrict__ U,
+                   const double* __restrict__ U0, double* __restrict__ Uout,
+                   const double* __restrict__ Fy, const double* __restrict__ Fz, Box b, FaceBox fy,
+                   FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
+                   double m1, double m2, double mc, double* __restrict__ clock) {
+    __shared__ double fprev[5][128];  // the x-face below the thread's next cell
+    // the update's operands of cell i (U0, U, the two y- and two z-faces), copied
+    // in while the thread computes x-face i+1; each thread reads only its own
+    __shared__ double opnd[30][128];
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
+    const int t = threadIdx.y * 32 + threadIdx.x;
+    const int x0 = blockIdx.z * NS_XMARCH_L, x1 = min(x0 + NS_XMARCH_L, b.nx);
+    if (k >= b.nz || j >= b.ny) return;  // no block barrier below
+    const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
+    const double m3 = mc * dt;
+    if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) {
+        clock[0] = dt;
+        clock[1] += dt;
+    }
+    // x-face a (between cells a-1 and a) of this thread's column
+    auto xface = [&](int a, double out[5]) {
+        long long step;
+        long long o0 = face_origin<0>(b, a, j, k, step);
+        double fL[5][5], fR[5][5], wa[5];
+        face_stencil<0, CHAR, PHYS, double>(W, U, b, c, o0, step, fL, fR, wa);
+        if constexpr (!CHAR)
+            face_comp<double, BORGES>(fL, fR, out);
+        else
+            face_char<0, PHYS, double, BORGES>(fL, fR, wa, c.gamma, c.inv_gm1, out);
+    };
+    const bool convz = flags & UPD_CONVZ;
+    // one face call site: the pass i = x0 - 1 only forms the first x-face
+    for (int i = x0 - 1; i < x1; i++) {
+        const long long o = b.at(i + NG, j + NG, k + NG);
+        if (i >= x0) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                cp_async8(&opnd[q][t], U0 + q * b.fstride + o);
+                cp_async8(&opnd[5 + q][t], U + q * b.fstride + o);
+                cp_async8(&opnd[10 + q][t], Fy + q * fy.fstride + fy.at(i, j, k));
+                cp_async8(&opnd[15 + q][t], Fy + q * fy.fstride + fy.at(i, j + 1, k));
+                if (convz) {
+                    cp_async8(&opnd[20 + q][t], Fz + q * fz.fstride + fz.at(i, j, k));
+                    cp_async8(&opnd[25 + q][t], Fz + q * fz.fstride + fz.at(i, j, k + 1));
+                }
+            }
+            cp_async_commit();
+        }
+        double f[5];
+        xface(i + 1, f);
+        if (i < x0) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) fprev[q][t] = f[q];
+            continue;
+        }
+        cp_async_wait_all();
+        // residual in k_update's order: x, y, z differences, then the viscous terms
+        double r[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            r[q] += (f[q] - fprev[q][t]) * c.inv_dx;
+            fprev[q][t] = f[q];
+            r[q] += (opnd[15 + q][t] - opnd[10 + q][t]) * c.inv_dy;
+            if (convz) r[q] += (opnd[25 + q][t] - opnd[20 + q][t]) * c.inv_dz;
+        }
+        if constexpr (H > 0) {
+            double rv[5] = {0, 0, 0, 0, 0};
+            if constexpr (PHYS)
+                viscous_physical<H, double>(W, b, c, i, j, k, rv);
+            else
+                viscous_reference<H, double>(W, b, c, i, j, k, rv);
+#pragma unroll
+            for (int q = 1; q < 5; q++) r[q] += rv[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 5; q++) Uout[q * b.fstride + o] = (opnd[q][t] * m1) + (opnd[5 + q][t] * m2) + (r[q] * m3);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host <-> device layout transposes (reference AoS [i][j][k][q], unpadded
 // (nx+6)(ny+6)(nz+6) x 5  <->  device SoA planes)
 
@@ -547,8 +644,8 @@ void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, un
     else k_min_dt<false><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, slot);
 }
 
-void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s) {
-    k_fill_prim<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c);
+void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s, double* Uhalo) {
+    k_fill_prim<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c, Uhalo);
 }
 
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
@@ -626,6 +723,35 @@ static void update_mode(const UpdateArgs& a, cudaStream_t s) {
 void launch_update(const UpdateArgs& a, cudaStream_t s) {
     if (a.mode == MODE_STAGE) update_mode<MODE_STAGE>(a, s);
     else update_mode<MODE_RHS>(a, s);
+}
+
+template <bool CHAR, bool BORGES, bool PHYS, int H>
+static void xupd_one(const UpdateArgs& a, cudaStream_t s) {
+    dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (a.b.nx + NS_XMARCH_L - 1) / NS_XMARCH_L);
+    k_xface_update<CHAR, BORGES, PHYS, H><<<grid, dim3(32, 4), 0, s>>>(
+        a.W, a.U, a.U0, a.Unext, (const double*)a.F[1], (const double*)a.F[2], a.b, a.fb[1], a.fb[2], a.c,
+        a.flags, a.slot, a.m1, a.m2, a.mc, a.clock);
+}
+
+template <bool CHAR, bool BORGES, bool PHYS>
+static void xupd_h(int h, const UpdateArgs& a, cudaStream_t s) {
+    switch (h) {
+        case 0: xupd_one<CHAR, BORGES, PHYS, 0>(a, s); break;
+        case 1: xupd_one<CHAR, BORGES, PHYS, 1>(a, s); break;
+        case 2: xupd_one<CHAR, BORGES, PHYS, 2>(a, s); break;
+        default: xupd_one<CHAR, BORGES, PHYS, 3>(a, s); break;
+    }
+}
+
+void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s) {
+    const int h = a.viscous ? a.c.order / 2 : 0;
+    if (chr) {
+        if (borges) { if (a.phys) xupd_h<true, true, true>(h, a, s); else xupd_h<true, true, false>(h, a, s); }
+        else { if (a.phys) xupd_h<true, false, true>(h, a, s); else xupd_h<true, false, false>(h, a, s); }
+    } else {
+        if (borges) { if (a.phys) xupd_h<false, true, true>(h, a, s); else xupd_h<false, true, false>(h, a, s); }
+        else { if (a.phys) xupd_h<false, false, true>(h, a, s); else xupd_h<false, false, false>(h, a, s); }
+    }
 }
 
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s) {

@@ -27,6 +27,7 @@ struct UpdateArgs {
     double m1, m2, mc;               // U = U0*m1 + U*m2 + R*(mc*dt)
     double* Rout;                    // MODE_RHS target (halo'd SoA)
     double* clock;                   // [last dt, accumulated time], updated once per step (nullable)
+    double* Unext;                   // launch_xface_update: the stage's output buffer
 };
 
 // per-face flags of the learned sensor (1 = characteristic-wise), FaceBox order
@@ -62,11 +63,15 @@ void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, 
 void launch_cons_all(const double* W, double* U, const Box& b, const Consts& c, cudaStream_t s);
 void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, unsigned long long* slot,
                    cudaStream_t s);
-void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s);
+// Uhalo (nullable) receives the same face-halo values as U
+void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s,
+                      double* Uhalo = nullptr);
 void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
                       const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
                       cudaStream_t s);
 void launch_update(const UpdateArgs& a, cudaStream_t s);
+// FP64 MODE_STAGE: x-faces + update in one march, U_out = a.Unext (a.F[0] unused)
+void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s);
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s);
 void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s);
 void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* acc, cudaStream_t s);

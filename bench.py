@@ -228,6 +228,10 @@ COMPUTE_PER_UNIT = {
     ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
     ("fp64_char", "update"): (316, 205, "fp64", "cell"),
     ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
+    # x-faces marched with the update: the x-face counts x (1 + 1/32 extra faces of
+    # each 32-cell march) plus the update's counts
+    ("fp64_char", "xface_update"): (1682, 1188, "fp64", "cell"),
+    ("fp64_comp", "xface_update"): (1311, 957, "fp64", "cell"),
     ("fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
     ("fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
 }
@@ -264,9 +268,12 @@ def rooflines(form, prof, n, peaks, fma):
            "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120,
            "stage_fused": cells * 120,
            # per-step sensor flags: U0 read once per axis, one byte per face written
-           "sensor": 3 * (cells * 40 + faces)}
+           "sensor": 3 * (cells * 40 + faces),
+           # x-faces + update: W and U (x stencils), the y- and z-face fluxes and U0
+           # read, U_out written
+           "xface_update": cells * 240}
     kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})",
-             "sensor": f"k_sensor_mask ({form})"}.get(
+             "sensor": f"k_sensor_mask ({form})", "xface_update": f"k_xface_update ({form})"}.get(
         dom, f"k_face_flux ({dom}, {form})" if dom.startswith("face") else dom)
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
