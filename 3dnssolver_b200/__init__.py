@@ -80,6 +80,7 @@ def load_library():
         "ns_sensor_predict": ([C, ctypes.c_longlong, fp, C, C], st),
         "ns_set_sensor_weights": ([C, fp], st),
         "ns_fma_peak": ([ctypes.c_int, dp], st),
+        "ns_get_dt": ([C, dp, dp], st),
     }
     for name, (args, res) in protos.items():
         f = getattr(L, name)
@@ -255,6 +256,12 @@ class Solver:
 
     def advance(self, nsteps):
         _check(self.lib.ns_advance(self.h, int(nsteps)), "ns_advance")
+
+    def get_dt(self):
+        """(dt of the last step, time accumulated over the steps taken)."""
+        dt, t = ctypes.c_double(), ctypes.c_double()
+        _check(self.lib.ns_get_dt(self.h, ctypes.byref(dt), ctypes.byref(t)), "ns_get_dt")
+        return dt.value, t.value
 
     def synchronize(self):
         _check(self.lib.ns_synchronize(self.h), "ns_synchronize")

@@ -31,9 +31,13 @@ def sources():
     return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu"))
 
 
+DRIVER_SRC = os.path.join(HERE, "driver", "ns_driver.cpp")
+DRIVER = os.path.join(LIBDIR, "ns_b200_driver")
+
+
 def _digest():
     h = hashlib.sha256()
-    for f in sorted(os.listdir(CSRC)) + [os.path.join(INCLUDE, "ns_b200.h")]:
+    for f in sorted(os.listdir(CSRC)) + [os.path.join(INCLUDE, "ns_b200.h"), DRIVER_SRC]:
         p = f if os.path.isabs(f) else os.path.join(CSRC, f)
         with open(p, "rb") as fh:
             h.update(p.encode() + fh.read())
@@ -45,7 +49,8 @@ def build(force=False, verbose=False):
     os.makedirs(LIBDIR, exist_ok=True)
     stamp = os.path.join(LIBDIR, ".digest")
     dig = _digest()
-    if not force and os.path.exists(LIB) and os.path.exists(stamp) and open(stamp).read() == dig:
+    if (not force and os.path.exists(LIB) and os.path.exists(DRIVER) and os.path.exists(stamp)
+            and open(stamp).read() == dig):
         return LIB
     objdir = os.path.join(LIBDIR, "_obj")
     os.makedirs(objdir, exist_ok=True)
@@ -70,9 +75,23 @@ def build(force=False, verbose=False):
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     os.replace(tmp, LIB)
+    build_driver()
     with open(stamp, "w") as fh:
         fh.write(dig)
     return LIB
+
+
+def build_driver():
+    """The input.xml-driven executable (the reference's main/Driver) over the C ABI."""
+    cxx = next((c for c in ("/usr/bin/g++", shutil.which("g++")) if c and os.path.exists(c)), None)
+    if cxx is None:
+        raise RuntimeError("g++ not found")
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", INCLUDE, DRIVER_SRC, "-L", LIBDIR, "-lns_b200",
+           "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{r.stdout}\n{r.stderr}")
+    return DRIVER
 
 
 if __name__ == "__main__":

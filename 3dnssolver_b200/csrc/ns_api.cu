@@ -668,6 +668,16 @@ ns_status ns_advance(ns_ctx* ctx, int nsteps) {
     return NS_OK;
 }
 
+ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    double h[2] = {0.0, 0.0};
+    NS_CUDA(cudaMemcpyAsync(h, ctx->clock, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (dt) *dt = h[0];
+    if (time) *time = h[1];
+    return NS_OK;
+}
+
 ns_status ns_synchronize(ns_ctx* ctx) {
     if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
     NS_CUDA(cudaStreamSynchronize(ctx->stream));

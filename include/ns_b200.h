@@ -153,6 +153,10 @@ NS_API ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out)
  * loop, src/driver.cpp:43-68, without host copies).  Asynchronous on the
  * context's stream; no host synchronisation inside. */
 NS_API ns_status ns_advance(ns_ctx* ctx, int nsteps);
+/* dt of the last step and the sum of dt over the steps taken (0 before the
+ * first step): TimeScheme::get_dt (src/time_scheme.hpp:31) plus the Driver's
+ * time accumulation (src/driver.cpp:54-58).  Waits for the context's stream. */
+NS_API ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time);
 /* Blocks until the context's stream is idle; NS_ERR_NONFINITE if
  * check_finite was requested and the state holds NaN/Inf. */
 NS_API ns_status ns_synchronize(ns_ctx* ctx);

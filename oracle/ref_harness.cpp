@@ -17,6 +17,10 @@
 //   MODE dt    : TimeScheme::set_dt on the input W; prints the dt
 //   MODE bench : steps= timed TimeScheme::step calls after warmup= untimed ones on
 //                a synthetic shear layer (in= optional); prints one JSON line
+//   MODE ic    : case= one of the test cases Driver::set_initial_condition
+//                dispatches (src/driver.cpp:107-141), set by the reference's own
+//                testcases.cpp on the zero-initialised Domain; writes W (halo'd AoS)
+//                to out= (pins the B200 driver's initial conditions)
 //   MODE dropin: (built with NS_WITH_B200) steps= steps of the same state three
 //                ways: the reference TimeScheme with its own operators, the
 //                reference TimeScheme with the B200 operators plugged in through
@@ -39,6 +43,7 @@
 #include "domain.hpp"
 #include "grid.hpp"
 #include "params.hpp"
+#include "testcases.hpp"
 #include "time_scheme.hpp" // also brings eq_of_state.hpp, whose include guard (EqOfState_hh vs EqOfSTate_hh) admits one inclusion only
 #ifdef NS_WITH_B200
 #include "ns_b200_adapters.hpp"
@@ -142,6 +147,31 @@ int main(int argc, char** argv) {
     Array4d& W = domain.get_NS_primitive_array();
     Array4d& U = domain.get_NS_conservative_array();
     const size_t nall = W.NX() * W.NY() * W.NZ() * W.NQ();
+
+    if (mode == "ic") {
+        const std::string c = S("case", "sod_x");
+        p.testcase = c;
+        if (c == "sod_x") testcases::sod_xdir(domain, grid, p);
+        else if (c == "sod_y") testcases::sod_ydir(domain, grid, p);
+        else if (c == "sod_z") testcases::sod_zdir(domain, grid, p);
+        else if (c == "case3") testcases::case3(domain, grid, p);
+        else if (c == "case4") testcases::case4(domain, grid, p);
+        else if (c == "case6") testcases::case6(domain, grid, p);
+        else if (c == "case12") testcases::case12(domain, grid, p);
+        else if (c == "case15") testcases::case15(domain, grid, p);
+        else if (c == "case17") testcases::case17(domain, grid, p);
+        else if (c == "shear_xy") testcases::shear_layer_xy(domain, grid, p);
+        else if (c == "shear_3d") testcases::shear_layer_3d(domain, grid, p);
+        else {
+            fprintf(stderr, "unknown case %s\n", c.c_str());
+            return 2;
+        }
+        FILE* f = fopen(S("out", "ic.bin").c_str(), "wb");
+        if (!f || fwrite(&W(0, 0, 0, 0), sizeof(double), nall, f) != nall) return 1;
+        fclose(f);
+        MPI_Finalize();
+        return 0;
+    }
 
     std::string in = S("in", "");
     if (!in.empty() && in != "shear") {
