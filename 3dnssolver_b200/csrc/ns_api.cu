@@ -222,8 +222,10 @@ static void prof_mark(ns_ctx* ctx, int cls) {
 }
 
 // face fluxes of the current (W, U) along every convected axis from first_dir on
-static ns_status faces(ns_ctx* ctx, int first_dir = 0) {
+// (U: the context's, or the stage input Uin)
+static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullptr) {
     const ns_params& p = ctx->p;
+    const double* U = Uin ? Uin : ctx->U;
     if (p.convection == NS_CONV_NONE) return NS_OK;
     int nd = p.dim == 3 ? 3 : 2;
     for (int d = first_dir; d < nd; d++) {
@@ -235,7 +237,7 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0) {
                             cudaGetErrorString(cudaGetLastError()));
         } else {
             launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
-                             phys(ctx), fp32(ctx), ctx->W, ctx->U, ctx->box, ctx->c, ctx->F[d],
+                             phys(ctx), fp32(ctx), ctx->W, U, ctx->box, ctx->c, ctx->F[d],
                              ctx->fb[d], ctx->stream);
             NS_TRY(check_launch(ctx, 1));
         }
@@ -338,43 +340,73 @@ static ns_status do_step_fused(ns_ctx* ctx) {
 static ns_status do_step(ns_ctx* ctx) {
     if (ctx->fused) return do_step_fused(ctx);
     cudaStream_t s = ctx->stream;
-    unsigned long long* cur = ctx->slot + ctx->parity;
-    NS_CUDA(cudaMemsetAsync(cur, 0xFF, sizeof(unsigned long long), s));
-    launch_step_begin(!ctx->w_valid, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s);
-    NS_TRY(check_launch(ctx, 1));
-    prof_mark(ctx, NS_PROF_STEP_BEGIN);
     // SSP-RK3 coefficients (time_scheme.cpp:36-38, 48-50, 60-62)
     const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
     const double m2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
     const double mc[3] = {-1.0, -(1. / 4.), -(2. / 3.)};
-    // FP64 with convection: y- and z-faces, then the x-faces marched together with
-    // the cell update into the second state buffer (the buffers swap each stage;
-    // the fill copies the stage input's face halos into the output buffer, so the
-    // state ends every stage, and the step, with the halos the reference holds)
-    const bool xfused = ctx->xfused;
-    for (int st = 0; st < 3; st++) {
-        launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s, xfused ? ctx->U2 : nullptr);
+    unsigned long long* cur = ctx->slot + ctx->parity;
+    if (!ctx->xfused) {
+        NS_CUDA(cudaMemsetAsync(cur, 0xFF, sizeof(unsigned long long), s));
+        launch_step_begin(!ctx->w_valid, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s);
         NS_TRY(check_launch(ctx, 1));
-        prof_mark(ctx, NS_PROF_FILL);
-        NS_TRY(faces(ctx, xfused ? 1 : 0));
-        UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
-        a.slot = cur;
-        a.m1 = m1[st];
-        a.m2 = m2[st];
-        a.mc = mc[st];
-        a.clock = (st == 0) ? ctx->clock : nullptr;
-        if (xfused) {
-            a.Unext = ctx->U2;
-            launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
+        prof_mark(ctx, NS_PROF_STEP_BEGIN);
+        for (int st = 0; st < 3; st++) {
+            launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
             NS_TRY(check_launch(ctx, 1));
-            std::swap(ctx->U, ctx->U2);
-            prof_mark(ctx, NS_PROF_XFACE_UPDATE);
-        } else {
+            prof_mark(ctx, NS_PROF_FILL);
+            NS_TRY(faces(ctx));
+            UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
+            a.slot = cur;
+            a.m1 = m1[st];
+            a.m2 = m2[st];
+            a.mc = mc[st];
+            a.clock = (st == 0) ? ctx->clock : nullptr;
             launch_update(a, s);
             NS_TRY(check_launch(ctx, 1));
             prof_mark(ctx, NS_PROF_UPDATE);
         }
+        ctx->u_valid = true;
+        ctx->w_valid = false;
+        ctx->steps++;
+        return NS_OK;
     }
+    // FP64 with convection: per stage the fill, the y- and z-faces, then the
+    // x-faces marched together with the cell update into the other buffer:
+    // U0 -> U -> U2 -> U (stage 1 reads the step's start U0 directly).  The
+    // fill copies the stage input's halos into the output buffer, so the step
+    // ends with the halos the reference's U holds.  The third stage also forms
+    // the next step's start (U0, and the CFL minimum in the other parity slot),
+    // so only the first step after a state change runs k_step_begin.
+    unsigned long long* nxt = ctx->slot + (ctx->parity ^ 1);
+    if (!ctx->fused_ready) {
+        NS_CUDA(cudaMemsetAsync(cur, 0xFF, sizeof(unsigned long long), s));
+        launch_step_begin(!ctx->w_valid, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s);
+        NS_TRY(check_launch(ctx, 1));
+        prof_mark(ctx, NS_PROF_STEP_BEGIN);
+    }
+    NS_CUDA(cudaMemsetAsync(nxt, 0xFF, sizeof(unsigned long long), s));
+    double* in[3] = {ctx->U0, ctx->U, ctx->U2};
+    double* out[3] = {ctx->U, ctx->U2, ctx->U};
+    for (int st = 0; st < 3; st++) {
+        launch_fill_prim(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
+        NS_TRY(check_launch(ctx, 1));
+        prof_mark(ctx, NS_PROF_FILL);
+        NS_TRY(faces(ctx, 1, in[st]));
+        UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
+        a.U = in[st];
+        a.Unext = out[st];
+        a.slot = cur;
+        a.slot_next = (st == 2) ? nxt : nullptr;
+        a.m1 = m1[st];
+        a.m2 = m2[st];
+        a.mc = mc[st];
+        a.clock = (st == 0) ? ctx->clock : nullptr;
+        launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
+        NS_TRY(check_launch(ctx, 1));
+        prof_mark(ctx, NS_PROF_XFACE_UPDATE);
+    }
+    ctx->parity ^= 1;
+    ctx->fused_ready = true;
     ctx->u_valid = true;
     ctx->w_valid = false;
     ctx->steps++;

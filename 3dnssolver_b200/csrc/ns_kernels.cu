@@ -439,21 +439,31 @@ __global__ void __launch_bounds__(128, NS_UPDATE_MINB) k_update(const double* __
 #ifndef NS_XMARCH_L
 #define NS_XMARCH_L 32
 #endif
-template <bool CHAR, bool BORGES, bool PHYS, int H>
+//
+// LAST (third stage): the next step's start as well -- W = prim(U_out) for its
+// CFL minimum (time_scheme.cpp:69, 98-136) into slot_next and U0 = cons(W)
+// (the W -> U round trip of time_scheme.cpp:124); U_out itself stays the raw
+// stage result, as the reference's U holds it between steps.  In the first stage U
+// and U0 are one buffer, only read; U0 is written in the third stage only, where
+// it is not U (so the restrict qualifiers hold).
+template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
 __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
-    k_xface_update(const double* __restrict__ W, const double* __restrict__ U,
-                   const double* __restrict__ U0, double* __restrict__ Uout,
+    k_xface_update(const double* __restrict__ W, const double* __restrict__ U, double* __restrict__ U0,
+                   double* __restrict__ Uout,
                    const double* __restrict__ Fy, const double* __restrict__ Fz, Box b, FaceBox fy,
                    FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
-                   double m1, double m2, double mc, double* __restrict__ clock) {
+                   unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
+                   double* __restrict__ clock) {
     __shared__ double fprev[5][128];  // the x-face below the thread's next cell
     // the update's operands of cell i (U0, U, the two y- and two z-faces), copied
     // in while the thread computes x-face i+1; each thread reads only its own
     __shared__ double opnd[30][128];
     const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
     const int t = threadIdx.y * 32 + threadIdx.x;
-    const int x0 = blockIdx.z * NS_XMARCH_L, x1 = min(x0 + NS_XMARCH_L, b.nx);
-    if (k >= b.nz || j >= b.ny) return;  // no block barrier below
+    const int x0 = blockIdx.z * NS_XMARCH_L;
+    // threads outside the grid march no cells but join the block reduction of LAST
+    const int x1 = (k < b.nz && j < b.ny) ? min(x0 + NS_XMARCH_L, b.nx) : x0 - 1;
+    double best = INFINITY;
     const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
     const double m3 = mc * dt;
     if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) {
@@ -515,9 +525,23 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
 #pragma unroll
             for (int q = 1; q < 5; q++) r[q] += rv[q];
         }
+        double un[5];
 #pragma unroll
-        for (int q = 0; q < 5; q++) Uout[q * b.fstride + o] = (opnd[q][t] * m1) + (opnd[5 + q][t] * m2) + (r[q] * m3);
+        for (int q = 0; q < 5; q++) {
+            un[q] = (opnd[q][t] * m1) + (opnd[5 + q][t] * m2) + (r[q] * m3);
+            Uout[q * b.fstride + o] = un[q];
+        }
+        if constexpr (LAST) {
+            double w[5], u0[5];
+            prim_from_cons(un, c.gm1, w);
+            const double d = PHYS ? local_dt_physical(w, c) : local_dt(w, c);
+            if (d < best) best = d;  // NaN never lowers the minimum (time_scheme.cpp:117)
+            cons_from_prim(w, c.inv_gm1, u0);
+#pragma unroll
+            for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u0[q];
+        }
     }
+    if constexpr (LAST) block_min_to(best, slot_next);
 }
 
 // ---------------------------------------------------------------------------
@@ -728,9 +752,14 @@ void launch_update(const UpdateArgs& a, cudaStream_t s) {
 template <bool CHAR, bool BORGES, bool PHYS, int H>
 static void xupd_one(const UpdateArgs& a, cudaStream_t s) {
     dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (a.b.nx + NS_XMARCH_L - 1) / NS_XMARCH_L);
-    k_xface_update<CHAR, BORGES, PHYS, H><<<grid, dim3(32, 4), 0, s>>>(
-        a.W, a.U, a.U0, a.Unext, (const double*)a.F[1], (const double*)a.F[2], a.b, a.fb[1], a.fb[2], a.c,
-        a.flags, a.slot, a.m1, a.m2, a.mc, a.clock);
+    if (a.slot_next)
+        k_xface_update<CHAR, BORGES, PHYS, H, true><<<grid, dim3(32, 4), 0, s>>>(
+            a.W, a.U, const_cast<double*>(a.U0), a.Unext, (const double*)a.F[1], (const double*)a.F[2], a.b,
+            a.fb[1], a.fb[2], a.c, a.flags, a.slot, a.slot_next, a.m1, a.m2, a.mc, a.clock);
+    else
+        k_xface_update<CHAR, BORGES, PHYS, H, false><<<grid, dim3(32, 4), 0, s>>>(
+            a.W, a.U, const_cast<double*>(a.U0), a.Unext, (const double*)a.F[1], (const double*)a.F[2], a.b,
+            a.fb[1], a.fb[2], a.c, a.flags, a.slot, nullptr, a.m1, a.m2, a.mc, a.clock);
 }
 
 template <bool CHAR, bool BORGES, bool PHYS>

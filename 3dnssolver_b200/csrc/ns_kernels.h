@@ -28,6 +28,8 @@ struct UpdateArgs {
     double* Rout;                    // MODE_RHS target (halo'd SoA)
     double* clock;                   // [last dt, accumulated time], updated once per step (nullable)
     double* Unext;                   // launch_xface_update: the stage's output buffer
+    unsigned long long* slot_next;   // launch_xface_update, third stage: the next step's CFL
+                                     // minimum (U0 then receives the next step's start)
 };
 
 // per-face flags of the learned sensor (1 = characteristic-wise), FaceBox order
