@@ -190,3 +190,35 @@ def test_gated_form_gains_over_component_wise():
     g, c, x = res["fp32_gated"], res["fp32_comp"], res["fp32_char"]
     assert 0.0 < g["sensor_fraction"] < 1.0
     assert g["rel_l2_rho"] < c["rel_l2_rho"] and g["rel_l2_rhoE"] < c["rel_l2_rhoE"], res
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order,weights,bc", [(2, 0, (N, P, P)), (4, 1, (P, N, P)), (6, 0, (N, N, N))])
+def test_gate_extremes_equal_the_ungated_forms(order, weights, bc):
+    """A network whose only nonzero parameter is the output bias flags every face
+    (b3 > 0) or none (b3 < 0): the gated stage kernel then reproduces ungated FP32
+    characteristic-wise / component-wise on every viscous order and weight type."""
+    shape = (20, 12, 10)
+    kw = dict(convection=pkg.CONV_WENO5_CHAR, diffusion_order=order, weights=weights, bc=bc, mu=0.02,
+              cfl=0.3, precision=pkg.PREC_FP32)
+    p = pkg.make_params(*shape, **kw)
+    W0 = wl.random_field(p, seed=31, smooth=False)
+
+    def run(b3=None, **extra):
+        q = pkg.make_params(*shape, **dict(kw, **extra))
+        with pkg.Solver(q) as s:
+            if b3 is not None:
+                w = np.zeros(pkg.SENSOR_NPARAMS, dtype=np.float32)
+                w[-1] = b3
+                s.set_sensor_weights(w)
+            s.upload_primitive(W0)
+            s.advance(3)
+            return s.download_conservative(), s.diagnostics()["sensor_fraction"]
+
+    U_char, _ = run()
+    U_comp, _ = run(convection=pkg.CONV_WENO5)
+    U_all, f_all = run(sensor=1, b3=10.0)
+    U_none, f_none = run(sensor=1, b3=-10.0)
+    assert f_all == 1.0 and f_none == 0.0
+    assert (rel_l2(interior(U_all), interior(U_char)) <= 1e-6).all()
+    assert (rel_l2(interior(U_none), interior(U_comp)) <= 1e-6).all()
