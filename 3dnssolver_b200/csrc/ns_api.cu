@@ -60,6 +60,8 @@ struct ns_ctx {
     double* U0 = nullptr;  // RK stage base (interior used)
     double* U2 = nullptr;  // second stage buffer of the fused paths
     bool xfused = false;   // FP64 steps: x-faces and update in one kernel (k_xface_update)
+    double* W2 = nullptr;  // its second W buffer (the next stage's W)
+    bool w_next_ready = false;  // with fused_ready: W holds prim(U0) for the next step's first stage
     double* R = nullptr;   // residual for the operator entry points (lazy)
     void* F[3] = {nullptr, nullptr, nullptr};
     double* stage = nullptr;              // host-layout staging (lazy)
@@ -387,14 +389,22 @@ static ns_status do_step(ns_ctx* ctx) {
     NS_CUDA(cudaMemsetAsync(nxt, 0xFF, sizeof(unsigned long long), s));
     double* in[3] = {ctx->U0, ctx->U, ctx->U2};
     double* out[3] = {ctx->U, ctx->U2, ctx->U};
+    // W's interior for a stage is the previous x-update's output (W and W2 swap
+    // each stage); the fill then covers the halos only.  A first stage without
+    // that output (after a state change or a download of W) fills all cells.
+    const bool w_ready = ctx->fused_ready && ctx->w_next_ready;
     for (int st = 0; st < 3; st++) {
-        launch_fill_prim(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
+        if (st == 0 && !w_ready)
+            launch_fill_prim(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
+        else
+            launch_fill_halo(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
         NS_TRY(check_launch(ctx, 1));
         prof_mark(ctx, NS_PROF_FILL);
         NS_TRY(faces(ctx, 1, in[st]));
         UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
         a.U = in[st];
         a.Unext = out[st];
+        a.Wnext = ctx->W2;
         a.slot = cur;
         a.slot_next = (st == 2) ? nxt : nullptr;
         a.m1 = m1[st];
@@ -403,10 +413,12 @@ static ns_status do_step(ns_ctx* ctx) {
         a.clock = (st == 0) ? ctx->clock : nullptr;
         launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
         NS_TRY(check_launch(ctx, 1));
+        std::swap(ctx->W, ctx->W2);
         prof_mark(ctx, NS_PROF_XFACE_UPDATE);
     }
     ctx->parity ^= 1;
     ctx->fused_ready = true;
+    ctx->w_next_ready = true;
     ctx->u_valid = true;
     ctx->w_valid = false;
     ctx->steps++;
@@ -418,6 +430,7 @@ static ns_status do_step(ns_ctx* ctx) {
 // the reference's W holds; its ghost cells then hold the filled values).
 static ns_status finalize_w(ns_ctx* ctx) {
     if (!ctx->w_valid) {
+        ctx->w_next_ready = false;  // W is about to hold prim(U), not the next stage's W
         if (ctx->halos_stale)
             launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, ctx->stream);
         else
@@ -488,6 +501,7 @@ void ns_destroy(ns_ctx* ctx) {
     cudaFree(ctx->U);
     cudaFree(ctx->U0);
     cudaFree(ctx->U2);
+    cudaFree(ctx->W2);
     cudaFree(ctx->R);
     for (int d = 0; d < 3; d++) cudaFree(ctx->F[d]);
     cudaFree(ctx->stage);
@@ -546,6 +560,7 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
     ctx->fused = (p->semantics == NS_SEM_REFERENCE) && p->precision == NS_PREC_FP32;
     ctx->xfused = !ctx->fused && p->precision == NS_PREC_FP64 && p->convection != NS_CONV_NONE;
     if (ctx->fused || ctx->xfused) A((void**)&ctx->U2, soa_bytes(ctx->box));
+    if (ctx->xfused) A((void**)&ctx->W2, soa_bytes(ctx->box));
     A((void**)&ctx->diag, 8 * sizeof(double));
     A((void**)&ctx->clock, 2 * sizeof(double));
     if (st == NS_OK) {

@@ -11,6 +11,8 @@
 // Per step: k_step_begin (dt reduction over W, then U = cons(W), U0 = U).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cfloat>
 #include <cmath>
 
@@ -24,7 +26,8 @@ namespace nsb {
 
 // ---------------------------------------------------------------------------
 // step begin: dt from W at the step start (TimeScheme::set_dt), then
-// U = cons(W) on every cell (time_scheme.cpp:124) and U0 = U (:126).
+// U = cons(W) on every cell (time_scheme.cpp:124) and U0 = U (:126), also on
+// every cell.
 // FROM_U: the state is U after the previous step; W = prim(U) first
 // (time_scheme.cpp:69).  Grid: (ceil(NZp/32), ceil(NY/4), NX).
 
@@ -57,10 +60,9 @@ __global__ void __launch_bounds__(128) k_step_begin(double* __restrict__ W, doub
         }
         cons_from_prim(w, c.inv_gm1, u);
 #pragma unroll
-        for (int q = 0; q < 5; q++) U[q * b.fstride + o] = u[q];
-        if (interior) {
-#pragma unroll
-            for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u[q];
+        for (int q = 0; q < 5; q++) {
+            U[q * b.fstride + o] = u[q];
+            U0[q * b.fstride + o] = u[q];  // all cells: the stages that start from U0 keep its edges
         }
     }
     block_min_to(best, slot);
@@ -150,6 +152,44 @@ __global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, doubl
 #pragma unroll
             for (int q = 0; q < 5; q++) Uhalo[q * b.fstride + o] = u[q];
         }
+    }
+    prim_from_cons(u, c.gm1, w);
+#pragma unroll
+    for (int q = 0; q < 5; q++) W[q * b.fstride + o] = w[q];
+}
+
+// Face halos only (the regions apply_boundary_conditions + communicate fill):
+// U there from its folded source, the same values into Uhalo, W = prim(U)
+// there.  The interior of W is the previous x-update's output.  Grid:
+// (ceil(3 * max face area / 128), 6 regions: x-, x+, y-, y+, z-, z+).
+__global__ void __launch_bounds__(128) k_fill_halo(double* __restrict__ W, double* __restrict__ U,
+                                                   Box b, Consts c, double* __restrict__ Uhalo) {
+    const int ax = blockIdx.y >> 1, hi = blockIdx.y & 1;
+    const long long t = (long long)blockIdx.x * 128 + threadIdx.x;
+    int i, j, k, layer;
+    if (ax == 0) {
+        if (t >= 3LL * b.ny * b.nz) return;
+        k = (int)(t % b.nz); j = (int)((t / b.nz) % b.ny); layer = (int)(t / ((long long)b.nz * b.ny));
+        i = hi ? b.nx + layer : layer - NG;
+    } else if (ax == 1) {
+        if (t >= 3LL * b.nx * b.nz) return;
+        k = (int)(t % b.nz); i = (int)((t / b.nz) % b.nx); layer = (int)(t / ((long long)b.nz * b.nx));
+        j = hi ? b.ny + layer : layer - NG;
+    } else {
+        if (t >= 3LL * b.nx * b.ny) return;
+        layer = (int)(t % 3); j = (int)((t / 3) % b.ny); i = (int)(t / (3LL * b.ny));
+        k = hi ? b.nz + layer : layer - NG;
+    }
+    const int si = ax == 0 ? fold(i, b.nx, c.periodic[0]) : i;
+    const int sj = ax == 1 ? fold(j, b.ny, c.periodic[1]) : j;
+    const int sk = ax == 2 ? fold(k, b.nz, c.periodic[2]) : k;
+    const long long o = b.at(i + NG, j + NG, k + NG), src = b.at(si + NG, sj + NG, sk + NG);
+    double u[5], w[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        u[q] = U[q * b.fstride + src];
+        U[q * b.fstride + o] = u[q];
+        if (Uhalo) Uhalo[q * b.fstride + o] = u[q];
     }
     prim_from_cons(u, c.gm1, w);
 #pragma unroll
@@ -449,7 +489,7 @@ __global__ void __launch_bounds__(128, NS_UPDATE_MINB) k_update(const double* __
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
 __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
     k_xface_update(const double* __restrict__ W, const double* __restrict__ U, double* __restrict__ U0,
-                   double* __restrict__ Uout,
+                   double* __restrict__ Uout, double* __restrict__ Wn,
                    const double* __restrict__ Fy, const double* __restrict__ Fz, Box b, FaceBox fy,
                    FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
                    unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
@@ -525,21 +565,24 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
 #pragma unroll
             for (int q = 1; q < 5; q++) r[q] += rv[q];
         }
-        double un[5];
+        double un[5], w[5];
 #pragma unroll
         for (int q = 0; q < 5; q++) {
             un[q] = (opnd[q][t] * m1) + (opnd[5 + q][t] * m2) + (r[q] * m3);
             Uout[q * b.fstride + o] = un[q];
         }
+        prim_from_cons(un, c.gm1, w);  // the next stage's W (conservative_to_primitive, time_scheme.cpp)
         if constexpr (LAST) {
-            double w[5], u0[5];
-            prim_from_cons(un, c.gm1, w);
+            double u0[5];
             const double d = PHYS ? local_dt_physical(w, c) : local_dt(w, c);
             if (d < best) best = d;  // NaN never lowers the minimum (time_scheme.cpp:117)
             cons_from_prim(w, c.inv_gm1, u0);
 #pragma unroll
             for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u0[q];
+            prim_from_cons(u0, c.gm1, w);  // the next step's first stage reads prim(U0)
         }
+#pragma unroll
+        for (int q = 0; q < 5; q++) Wn[q * b.fstride + o] = w[q];
     }
     if constexpr (LAST) block_min_to(best, slot_next);
 }
@@ -668,6 +711,11 @@ void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, un
     else k_min_dt<false><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, slot);
 }
 
+void launch_fill_halo(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s, double* Uhalo) {
+    const long long area = std::max(std::max((long long)b.ny * b.nz, (long long)b.nx * b.nz), (long long)b.nx * b.ny);
+    k_fill_halo<<<dim3((unsigned)((3 * area + 127) / 128), 6), 128, 0, s>>>(W, U, b, c, Uhalo);
+}
+
 void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s, double* Uhalo) {
     k_fill_prim<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c, Uhalo);
 }
@@ -754,12 +802,12 @@ static void xupd_one(const UpdateArgs& a, cudaStream_t s) {
     dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (a.b.nx + NS_XMARCH_L - 1) / NS_XMARCH_L);
     if (a.slot_next)
         k_xface_update<CHAR, BORGES, PHYS, H, true><<<grid, dim3(32, 4), 0, s>>>(
-            a.W, a.U, const_cast<double*>(a.U0), a.Unext, (const double*)a.F[1], (const double*)a.F[2], a.b,
-            a.fb[1], a.fb[2], a.c, a.flags, a.slot, a.slot_next, a.m1, a.m2, a.mc, a.clock);
+            a.W, a.U, const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1], (const double*)a.F[2],
+            a.b, a.fb[1], a.fb[2], a.c, a.flags, a.slot, a.slot_next, a.m1, a.m2, a.mc, a.clock);
     else
         k_xface_update<CHAR, BORGES, PHYS, H, false><<<grid, dim3(32, 4), 0, s>>>(
-            a.W, a.U, const_cast<double*>(a.U0), a.Unext, (const double*)a.F[1], (const double*)a.F[2], a.b,
-            a.fb[1], a.fb[2], a.c, a.flags, a.slot, nullptr, a.m1, a.m2, a.mc, a.clock);
+            a.W, a.U, const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1], (const double*)a.F[2],
+            a.b, a.fb[1], a.fb[2], a.c, a.flags, a.slot, nullptr, a.m1, a.m2, a.mc, a.clock);
 }
 
 template <bool CHAR, bool BORGES, bool PHYS>

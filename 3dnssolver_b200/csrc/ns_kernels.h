@@ -28,6 +28,7 @@ struct UpdateArgs {
     double* Rout;                    // MODE_RHS target (halo'd SoA)
     double* clock;                   // [last dt, accumulated time], updated once per step (nullable)
     double* Unext;                   // launch_xface_update: the stage's output buffer
+    double* Wnext;                   // launch_xface_update: the next stage's W (interior)
     unsigned long long* slot_next;   // launch_xface_update, third stage: the next step's CFL
                                      // minimum (U0 then receives the next step's start)
 };
@@ -65,6 +66,9 @@ void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, 
 void launch_cons_all(const double* W, double* U, const Box& b, const Consts& c, cudaStream_t s);
 void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, unsigned long long* slot,
                    cudaStream_t s);
+// face halos of U and W only (the interior of W is already the stage's)
+void launch_fill_halo(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s,
+                      double* Uhalo = nullptr);
 // Uhalo (nullable) receives the same face-halo values as U
 void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s,
                       double* Uhalo = nullptr);

@@ -270,8 +270,8 @@ def rooflines(form, prof, n, peaks, fma):
            # per-step sensor flags: U0 read once per axis, one byte per face written
            "sensor": 3 * (cells * 40 + faces),
            # x-faces + update: W and U (x stencils), the y- and z-face fluxes and U0
-           # read, U_out written
-           "xface_update": cells * 240}
+           # read, U_out and the next stage's W written
+           "xface_update": cells * 280}
     kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})",
              "sensor": f"k_sensor_mask ({form})", "xface_update": f"k_xface_update ({form})"}.get(
         dom, f"k_face_flux ({dom}, {form})" if dom.startswith("face") else dom)
