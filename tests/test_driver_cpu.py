@@ -86,3 +86,34 @@ def test_initial_conditions_match_the_reference_bitwise(tmp_path, case):
     ref = z[case].ravel()
     assert w.shape == ref.shape
     np.testing.assert_array_equal(w.view(np.int64), ref.view(np.int64))
+
+
+def test_restart_file_checks(tmp_path):
+    """A checkpoint of the wrong size or without its .time file is refused before any device work."""
+    xml = driver_xml(n=(4, 3, 2))
+    good = np.zeros(4 * 3 * 2 * 5)
+    (tmp_path / "short_p_0.dat").write_bytes(good[:-1].tobytes())
+    (tmp_path / "short_p_0.time").write_text("0.5 10\n")
+    r = run_driver(tmp_path, xml, "--restart", tmp_path / "short_p_0.dat")
+    assert r.returncode == 4 and "fewer than" in r.stderr
+    (tmp_path / "long_p_0.dat").write_bytes(np.zeros(good.size + 1).tobytes())
+    (tmp_path / "long_p_0.time").write_text("0.5 10\n")
+    r = run_driver(tmp_path, xml, "--restart", tmp_path / "long_p_0.dat")
+    assert r.returncode == 4 and "more than" in r.stderr
+    (tmp_path / "notime_p_0.dat").write_bytes(good.tobytes())
+    r = run_driver(tmp_path, xml, "--restart", tmp_path / "notime_p_0.dat")
+    assert r.returncode == 4 and ".time" in r.stderr
+
+
+def test_restart_dump_reproduces_the_checkpoint(tmp_path):
+    """--restart with --dump-ic writes the checkpoint's interior into the halo'd layout."""
+    n = (4, 3, 2)
+    xml = driver_xml(n=n)
+    W = np.random.default_rng(3).standard_normal((n[0], n[1], n[2], 5))
+    (tmp_path / "f_p_0.dat").write_bytes(W.tobytes())
+    (tmp_path / "f_p_0.time").write_text("1.25 7\n")
+    r = run_driver(tmp_path, xml, "--restart", tmp_path / "f_p_0.dat", "--dump-ic", tmp_path / "w.bin")
+    assert r.returncode == 0, r.stderr
+    full = np.fromfile(tmp_path / "w.bin").reshape(n[0] + 6, n[1] + 6, n[2] + 6, 5)
+    np.testing.assert_array_equal(full[3:-3, 3:-3, 3:-3], W)
+    assert not full[:3].any() and not full[-3:].any()
