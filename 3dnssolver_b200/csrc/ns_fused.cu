@@ -218,12 +218,26 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
         cp_async_wait_all();
         T* P = plane(i);
         for (int e = rotated(tid, 5); e < M::NP; e += FT) {
-            double u[5], w[5];
+            if constexpr (sizeof(T) == 4) {
+                // the FP32 form's W in FP32 arithmetic from the FP64 state
+                float u[5];
 #pragma unroll
-            for (int q = 0; q < 5; q++) u[q] = S[q * M::NP + e];
-            prim_from_cons(u, c.gm1, w);
+                for (int q = 0; q < 5; q++) u[q] = float(S[q * M::NP + e]);
+                const float ir = __fdividef(1.f, u[0]);
+                const float vx = u[2] * ir, vy = u[3] * ir, vz = u[4] * ir;
+                P[e] = u[0];
+                P[M::NP + e] = float(c.gm1) * (u[1] - 0.5f * u[0] * (vx * vx + vy * vy + vz * vz));
+                P[2 * M::NP + e] = vx;
+                P[3 * M::NP + e] = vy;
+                P[4 * M::NP + e] = vz;
+            } else {
+                double u[5], w[5];
 #pragma unroll
-            for (int q = 0; q < 5; q++) P[q * M::NP + e] = T(w[q]);
+                for (int q = 0; q < 5; q++) u[q] = S[q * M::NP + e];
+                prim_from_cons(u, c.gm1, w);
+#pragma unroll
+                for (int q = 0; q < 5; q++) P[q * M::NP + e] = T(w[q]);
+            }
         }
     };
     auto load_plane = [&](int i) {
