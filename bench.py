@@ -228,10 +228,9 @@ COMPUTE_PER_UNIT = {
     ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
     ("fp64_char", "update"): (316, 205, "fp64", "cell"),
     ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
-    # x-faces marched with the update: the x-face counts x (1 + 1/32 extra faces of
-    # each 32-cell march) plus the update's counts
-    ("fp64_char", "xface_update"): (1682, 1188, "fp64", "cell"),
-    ("fp64_comp", "xface_update"): (1311, 957, "fp64", "cell"),
+    # x-faces marched with the update (first two stages; measured per cell)
+    ("fp64_char", "xface_update"): (1630, 1147, "fp64", "cell"),
+    ("fp64_comp", "xface_update"): (1286, 923, "fp64", "cell"),
     ("fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
     ("fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
 }
@@ -241,6 +240,7 @@ TRAFFIC_PER_UNIT = {
     ("fp64_char", "face_x"): 120.4, ("fp64_char", "face_y"): 118.6, ("fp64_char", "face_z"): 113.6,
     ("fp64_comp", "face_x"): 119.7, ("fp64_comp", "face_y"): 118.7, ("fp64_comp", "face_z"): 113.3,
     ("fp64_char", "update"): 283.7, ("fp64_comp", "update"): 283.7,
+    ("fp64_char", "xface_update"): 311.9, ("fp64_comp", "xface_update"): 306.9,
 }
 
 
