@@ -168,24 +168,19 @@ __device__ __forceinline__ void split_cell(int s, const T w[5], const T u[5], T 
     }
 }
 
-// stencil load + Euler flux + Lax-Friedrichs split; wa receives the face
+// Euler flux + Lax-Friedrichs split of a 6-cell stencil whose cells the loader
+// supplies: ld(s, w, u) gives W and U of stencil cell s; wa receives the face
 // average of W (characteristic form only)
-template <int DIR, bool CHAR, bool PHYS, typename T>
-__device__ __forceinline__ void face_stencil(const double* __restrict__ W, const double* __restrict__ U,
-                                             const Box& b, const Consts& c, long long o0,
-                                             long long step, T fL[5][5], T fR[5][5], T wa[5]) {
-    const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1), half = T(0.5);
-    const T hg = half * gamma * inv_gm1;  // gamma/(2(gamma-1))
+template <int DIR, bool CHAR, bool PHYS, typename T, typename Loader>
+__device__ __forceinline__ void face_stencil_from(Loader ld, const Consts& c, T fL[5][5], T fR[5][5],
+                                                  T wa[5]) {
+    const T gamma = T(c.gamma), half = T(0.5);
+    const T hg = half * gamma * T(c.inv_gm1);  // gamma/(2(gamma-1))
     if constexpr (!PHYS) {
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            long long o = o0 + s * step;
             T w[5], u[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) {
-                w[q] = T(W[q * b.fstride + o]);
-                u[q] = T(U[q * b.fstride + o]);
-            }
+            ld(s, w, u);
             split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
         }
     } else {
@@ -194,13 +189,8 @@ __device__ __forceinline__ void face_stencil(const double* __restrict__ W, const
         T Fc[6][5], Uc[6][5], halpha = T(0);
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            long long o = o0 + s * step;
             T w[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) {
-                w[q] = T(W[q * b.fstride + o]);
-                Uc[s][q] = T(U[q * b.fstride + o]);
-            }
+            ld(s, w, Uc[s]);
             if constexpr (CHAR) {
                 if (s == 2) {
 #pragma unroll
@@ -223,6 +213,22 @@ __device__ __forceinline__ void face_stencil(const double* __restrict__ W, const
                 if (s >= 1) fR[q][s - 1] = Fc[s][q] - halpha * Uc[s][q];
             }
     }
+}
+
+// stencil load from the device state + Euler flux + Lax-Friedrichs split
+template <int DIR, bool CHAR, bool PHYS, typename T>
+__device__ __forceinline__ void face_stencil(const double* __restrict__ W, const double* __restrict__ U,
+                                             const Box& b, const Consts& c, long long o0,
+                                             long long step, T fL[5][5], T fR[5][5], T wa[5]) {
+    auto ld = [&](int s, T w[5], T u[5]) {
+        const long long o = o0 + s * step;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            w[q] = T(W[q * b.fstride + o]);
+            u[q] = T(U[q * b.fstride + o]);
+        }
+    };
+    face_stencil_from<DIR, CHAR, PHYS, T>(ld, c, fL, fR, wa);
 }
 
 // component-wise: f_q = WENO5_left(fL_q) + WENO5_right(fR_q)   (weno-5.cpp:96-114)

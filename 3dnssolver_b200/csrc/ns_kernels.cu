@@ -510,12 +510,21 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
         clock[0] = dt;
         clock[1] += dt;
     }
-    // x-face a (between cells a-1 and a) of this thread's column
+    // x-face a (between cells a-1 and a) of this thread's column.  The stencil
+    // reads W only and forms U = cons(W) (rounding-level difference from the
+    // stage's U): half the cached working set of a march, which keeps the
+    // re-read stencil cells in L1.
     auto xface = [&](int a, double out[5]) {
         long long step;
-        long long o0 = face_origin<0>(b, a, j, k, step);
+        const long long o0 = face_origin<0>(b, a, j, k, step);
+        auto ld = [&](int s, double w[5], double u[5]) {
+            const long long os = o0 + s * step;
+#pragma unroll
+            for (int q = 0; q < 5; q++) w[q] = W[q * b.fstride + os];
+            cons_from_prim(w, c.inv_gm1, u);
+        };
         double fL[5][5], fR[5][5], wa[5];
-        face_stencil<0, CHAR, PHYS, double>(W, U, b, c, o0, step, fL, fR, wa);
+        face_stencil_from<0, CHAR, PHYS, double>(ld, c, fL, fR, wa);
         if constexpr (!CHAR)
             face_comp<double, BORGES>(fL, fR, out);
         else
