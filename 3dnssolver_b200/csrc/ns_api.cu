@@ -225,7 +225,7 @@ static void prof_mark(ns_ctx* ctx, int cls) {
 
 // face fluxes of the current (W, U) along every convected axis from first_dir on
 // (U: the context's, or the stage input Uin)
-static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullptr) {
+static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullptr, bool w_only = false) {
     const ns_params& p = ctx->p;
     const double* U = Uin ? Uin : ctx->U;
     if (p.convection == NS_CONV_NONE) return NS_OK;
@@ -240,7 +240,7 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullp
         } else {
             launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
                              phys(ctx), fp32(ctx), ctx->W, U, ctx->box, ctx->c, ctx->F[d],
-                             ctx->fb[d], ctx->stream);
+                             ctx->fb[d], ctx->stream, w_only);
             NS_TRY(check_launch(ctx, 1));
         }
         prof_mark(ctx, NS_PROF_FACE_X + d);
@@ -400,7 +400,7 @@ static ns_status do_step(ns_ctx* ctx) {
             launch_fill_halo(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
         NS_TRY(check_launch(ctx, 1));
         prof_mark(ctx, NS_PROF_FILL);
-        NS_TRY(faces(ctx, 1, in[st]));
+        NS_TRY(faces(ctx, 1, in[st], true));  // W = prim(U) here: the stencils read W only
         UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
         a.U = in[st];
         a.Unext = out[st];

@@ -221,7 +221,9 @@ struct FaceMinBlocks {
                                                 : (CHAR ? NS_FACE_MINB_F32CHAR : NS_FACE_MINB_F32COMP);
 };
 
-template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
+// WONLY (time steps, where W = prim(U)): the stencil reads W only and forms U =
+// cons(W), half the loads; operator calls read the caller's U as given.
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY = false>
 __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
     k_face_flux(const double* __restrict__ W, const double* __restrict__ U, Box b, Consts c,
                 TF* __restrict__ F, FaceBox fb) {
@@ -232,7 +234,17 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
     long long step;
     long long o0 = face_origin<DIR>(b, aa, bb, kk, step);
     T fL[5][5], fR[5][5], wa[5];
-    face_stencil<DIR, CHAR, PHYS, T>(W, U, b, c, o0, step, fL, fR, wa);
+    if constexpr (WONLY) {
+        auto ld = [&](int s, T w[5], T u[5]) {
+            const long long os = o0 + s * step;
+#pragma unroll
+            for (int q = 0; q < 5; q++) w[q] = W[q * b.fstride + os];
+            cons_from_prim(w, c.inv_gm1, u);
+        };
+        face_stencil_from<DIR, CHAR, PHYS, T>(ld, c, fL, fR, wa);
+    } else {
+        face_stencil<DIR, CHAR, PHYS, T>(W, U, b, c, o0, step, fL, fR, wa);
+    }
     T out[5];
     if constexpr (!CHAR)
         face_comp<T, BORGES>(fL, fR, out);
@@ -731,44 +743,51 @@ void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaS
 
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
 static void face_one(const double* W, const double* U, const Box& b, const Consts& c, void* F,
-                     const FaceBox& fb, cudaStream_t s) {
+                     const FaceBox& fb, cudaStream_t s, bool w_only) {
     dim3 grid((fb.n2 + 31) / 32, (fb.n1 + 3) / 4, fb.n0);
+    if constexpr (sizeof(T) == 8 && DIR > 0) {
+        if (w_only) {
+            k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF, true><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
+            return;
+        }
+    }
     k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
 }
 
 template <int DIR, typename T, typename TF>
 static void face_dispatch(bool chr, bool borges, bool phys, const double* W, const double* U,
-                          const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s) {
+                          const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s,
+                          bool w_only) {
     if (chr) {
         if (borges) {
-            if (phys) face_one<DIR, true, true, true, T, TF>(W, U, b, c, F, fb, s);
-            else face_one<DIR, true, true, false, T, TF>(W, U, b, c, F, fb, s);
+            if (phys) face_one<DIR, true, true, true, T, TF>(W, U, b, c, F, fb, s, w_only);
+            else face_one<DIR, true, true, false, T, TF>(W, U, b, c, F, fb, s, w_only);
         } else {
-            if (phys) face_one<DIR, true, false, true, T, TF>(W, U, b, c, F, fb, s);
-            else face_one<DIR, true, false, false, T, TF>(W, U, b, c, F, fb, s);
+            if (phys) face_one<DIR, true, false, true, T, TF>(W, U, b, c, F, fb, s, w_only);
+            else face_one<DIR, true, false, false, T, TF>(W, U, b, c, F, fb, s, w_only);
         }
     } else {
         if (borges) {
-            if (phys) face_one<DIR, false, true, true, T, TF>(W, U, b, c, F, fb, s);
-            else face_one<DIR, false, true, false, T, TF>(W, U, b, c, F, fb, s);
+            if (phys) face_one<DIR, false, true, true, T, TF>(W, U, b, c, F, fb, s, w_only);
+            else face_one<DIR, false, true, false, T, TF>(W, U, b, c, F, fb, s, w_only);
         } else {
-            if (phys) face_one<DIR, false, false, true, T, TF>(W, U, b, c, F, fb, s);
-            else face_one<DIR, false, false, false, T, TF>(W, U, b, c, F, fb, s);
+            if (phys) face_one<DIR, false, false, true, T, TF>(W, U, b, c, F, fb, s, w_only);
+            else face_one<DIR, false, false, false, T, TF>(W, U, b, c, F, fb, s, w_only);
         }
     }
 }
 
 void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
                       const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
-                      cudaStream_t s) {
+                      cudaStream_t s, bool w_only) {
     if (fp32) {
-        if (dir == 0) face_dispatch<0, float, float>(chr, borges, phys, W, U, b, c, F, fb, s);
-        else if (dir == 1) face_dispatch<1, float, float>(chr, borges, phys, W, U, b, c, F, fb, s);
-        else face_dispatch<2, float, float>(chr, borges, phys, W, U, b, c, F, fb, s);
+        if (dir == 0) face_dispatch<0, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false);
+        else if (dir == 1) face_dispatch<1, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false);
+        else face_dispatch<2, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false);
     } else {
-        if (dir == 0) face_dispatch<0, double, double>(chr, borges, phys, W, U, b, c, F, fb, s);
-        else if (dir == 1) face_dispatch<1, double, double>(chr, borges, phys, W, U, b, c, F, fb, s);
-        else face_dispatch<2, double, double>(chr, borges, phys, W, U, b, c, F, fb, s);
+        if (dir == 0) face_dispatch<0, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only);
+        else if (dir == 1) face_dispatch<1, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only);
+        else face_dispatch<2, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only);
     }
 }
 

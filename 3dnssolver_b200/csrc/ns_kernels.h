@@ -72,9 +72,10 @@ void launch_fill_halo(double* W, double* U, const Box& b, const Consts& c, cudaS
 // Uhalo (nullable) receives the same face-halo values as U
 void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s,
                       double* Uhalo = nullptr);
+// w_only (FP64 y- and z-faces of a time step, where W = prim(U)): U = cons(W)
 void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
                       const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
-                      cudaStream_t s);
+                      cudaStream_t s, bool w_only = false);
 void launch_update(const UpdateArgs& a, cudaStream_t s);
 // FP64 MODE_STAGE: x-faces + update in one march, U_out = a.Unext (a.F[0] unused)
 void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s);
