@@ -207,6 +207,84 @@ __device__ __forceinline__ void mlp_forward(const MlpSmem& m, const __nv_bfloat1
     }
 }
 
+// Inference-only forward for the per-step flags: GELU on packed BF16 pairs
+// (tanh.approx.bf16x2 and bf16x2 FMAs: half the special-function and FMA
+// instructions of the FP32 GELU).  The layer-1 activations feed layer 2 as
+// BF16 either way; the layer-2 activations are widened to FP32 for the output
+// dot product.  Training and ns_sensor_predict use the FP32 GELU above.
+__device__ __forceinline__ __nv_bfloat162 tanh_bf16x2(__nv_bfloat162 x) {
+    uint32_t xi = *reinterpret_cast<uint32_t*>(&x), yi;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(yi) : "r"(xi));
+    return *reinterpret_cast<__nv_bfloat162*>(&yi);
+}
+__device__ __forceinline__ __nv_bfloat162 gelu_bf16x2(float a, float b) {
+    const __nv_bfloat162 x = __floats2bfloat162_rn(a, b);
+    const __nv_bfloat162 c0 = __float2bfloat162_rn(0.7978845608028654f);
+    const __nv_bfloat162 c1 = __float2bfloat162_rn(0.7978845608028654f * 0.044715f);
+    const __nv_bfloat162 half = __float2bfloat162_rn(0.5f);
+    const __nv_bfloat162 u = __hmul2(x, __hfma2(__hmul2(x, x), c1, c0));  // k0 (x + k1 x^3)
+    const __nv_bfloat162 h = __hmul2(half, x);
+    return __hfma2(h, tanh_bf16x2(u), h);
+}
+
+__device__ __forceinline__ void mlp_logits_fast(const MlpSmem& m, const __nv_bfloat16* X, float lg[2][2]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+        uint32_t a[2][4];
+        afrag(X, mt, 0, g, q, a[0]);
+        afrag(X, mt, 1, g, q, a[1]);
+        float z1[4][4];
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            float* d = z1[nt];
+            float bl = m.b1[8 * nt + 2 * q], bh = m.b1[8 * nt + 2 * q + 1];
+            d[0] = bl; d[1] = bh; d[2] = bl; d[3] = bh;
+#pragma unroll
+            for (int kt = 0; kt < 2; kt++) {
+                uint32_t b[2];
+                bfrag(m.W1, nt, kt, g, q, b);
+                mma16816(d, a[kt], b);
+            }
+        }
+        uint32_t h1a[2][4];
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const float* c0 = z1[2 * t];
+            const float* c1 = z1[2 * t + 1];
+            __nv_bfloat162 v;
+            v = gelu_bf16x2(c0[0], c0[1]); h1a[t][0] = *reinterpret_cast<uint32_t*>(&v);
+            v = gelu_bf16x2(c0[2], c0[3]); h1a[t][1] = *reinterpret_cast<uint32_t*>(&v);
+            v = gelu_bf16x2(c1[0], c1[1]); h1a[t][2] = *reinterpret_cast<uint32_t*>(&v);
+            v = gelu_bf16x2(c1[2], c1[3]); h1a[t][3] = *reinterpret_cast<uint32_t*>(&v);
+        }
+        float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) {
+            float d[4];
+            float bl = m.b2[8 * nt + 2 * q], bh = m.b2[8 * nt + 2 * q + 1];
+            d[0] = bl; d[1] = bh; d[2] = bl; d[3] = bh;
+#pragma unroll
+            for (int kt = 0; kt < 2; kt++) {
+                uint32_t b[2];
+                bfrag(m.W2, nt, kt, g, q, b);
+                mma16816(d, h1a[kt], b);
+            }
+            const float wl = m.w3[8 * nt + 2 * q], wh = m.w3[8 * nt + 2 * q + 1];
+            const float2 r0 = __bfloat1622float2(gelu_bf16x2(d[0], d[1]));
+            const float2 r1 = __bfloat1622float2(gelu_bf16x2(d[2], d[3]));
+            s0 = fmaf(r0.x, wl, fmaf(r0.y, wh, s0));
+            s1 = fmaf(r1.x, wl, fmaf(r1.y, wh, s1));
+        }
+        s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+        s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+        lg[mt][0] = s0 + m.b3;
+        lg[mt][1] = s1 + m.b3;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // features
 
@@ -649,14 +727,14 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const double* __restrict__ 
 #pragma unroll
         for (int e = 0; e < XS; e++) X[lane * XS + e] = __float2bfloat16(e < SF ? feat[e] : 0.f);
         __syncwarp();
-        MlpFwd f;
-        mlp_forward(m, X, f);
+        float lgs[2][2];
+        mlp_logits_fast(m, X, lgs);
         float lg = 0.f;
 #pragma unroll
         for (int mt = 0; mt < 2; mt++)
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                float v = __shfl_sync(0xffffffffu, f.lg[mt][h], 4 * (lane & 7));
+                float v = __shfl_sync(0xffffffffu, lgs[mt][h], 4 * (lane & 7));
                 if ((lane >> 4) == mt && ((lane >> 3) & 1) == h) lg = v;
             }
         const bool fire = live && lg > logit_thr;
