@@ -678,8 +678,27 @@ __global__ void __launch_bounds__(128) k_face_gated(const double* __restrict__ W
 // the step's start state U0 (W = prim(U0) at boundary-folded cells, the
 // stage kernel's own halo rule), one byte per face (1 = characteristic-wise)
 
+// rho, p, u, v, w of every interior cell in FP32 (what the flags' features read),
+// SoA planes of nx*ny*nz floats, from the step's start state U0
+__global__ void __launch_bounds__(128) k_sensor_prims(const double* __restrict__ U0, Box b, Consts c,
+                                                      float* __restrict__ prim) {
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, i = blockIdx.z;
+    if (k >= b.nz || j >= b.ny) return;
+    const long long o = b.at(i + NG, j + NG, k + NG);
+    const long long n = (long long)b.nx * b.ny * b.nz, e = ((long long)i * b.ny + j) * b.nz + k;
+    float u[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) u[q] = float(U0[q * b.fstride + o]);
+    const float ir = __fdividef(1.f, u[0]);
+    prim[e] = u[0];
+    prim[n + e] = float(c.gm1) * (u[1] - 0.5f * ir * (u[2] * u[2] + u[3] * u[3] + u[4] * u[4]));
+    prim[2 * n + e] = u[2] * ir;
+    prim[3 * n + e] = u[3] * ir;
+    prim[4 * n + e] = u[4] * ir;
+}
+
 template <int DIR>
-__global__ void __launch_bounds__(128) k_sensor_mask(const double* __restrict__ U0, Box b, Consts c,
+__global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ prim, Box b, Consts c,
                                                      FaceBox fb, const float* __restrict__ w,
                                                      float logit_thr, unsigned char* __restrict__ mask,
                                                      unsigned long long* __restrict__ flagged) {
@@ -688,7 +707,7 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const double* __restrict__ 
     const int warp = threadIdx.y, lane = threadIdx.x;
     mlp_load(m, w, false);  // once per block: the grid strides over 32 x 4 tiles of faces
     __syncthreads();
-    const float gm1 = float(c.gm1), gamma = float(c.gamma);
+    const float gamma = float(c.gamma);
     const int t2 = (fb.n2 + 31) / 32, t1 = (fb.n1 + 3) / 4;
     const long long tiles = (long long)t2 * t1 * fb.n0;
     __nv_bfloat16* X = Xs[warp];
@@ -701,7 +720,8 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const double* __restrict__ 
         float feat[SF];
         if (live) {
             // face aa lies between cells aa-1 and aa along DIR: stencil aa-3..aa+2;
-            // rho, p and u_n in FP32 (the network reads BF16 features)
+            // rho, p and u_n in FP32 from the step's primitive planes
+            const long long n = (long long)b.nx * b.ny * b.nz;
             float rho[6], p[6], un[6];
 #pragma unroll
             for (int s = 0; s < 6; s++) {
@@ -709,14 +729,10 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const double* __restrict__ 
                 if (DIR == 0) i = fold(aa - 3 + s, b.nx, c.periodic[0]);
                 if (DIR == 1) j = fold(bb - 3 + s, b.ny, c.periodic[1]);
                 if (DIR == 2) k = fold(kk - 3 + s, b.nz, c.periodic[2]);
-                const long long o = b.at(i + NG, j + NG, k + NG);
-                float u[5];
-#pragma unroll
-                for (int q = 0; q < 5; q++) u[q] = float(U0[q * b.fstride + o]);
-                const float ir = __fdividef(1.f, u[0]);
-                rho[s] = u[0];
-                un[s] = u[2 + DIR] * ir;
-                p[s] = gm1 * (u[1] - 0.5f * ir * (u[2] * u[2] + u[3] * u[3] + u[4] * u[4]));
+                const long long e = ((long long)i * b.ny + j) * b.nz + k;
+                rho[s] = prim[e];
+                p[s] = prim[n + e];
+                un[s] = prim[(2 + DIR) * n + e];
             }
             face_features<float>(rho, p, un, gamma, feat);
         } else {
@@ -751,18 +767,20 @@ struct SensorState {
     float* w = nullptr;                    // FP32 parameters on the device
     unsigned long long* flagged = nullptr;  // faces flagged since creation
     unsigned char* mask[3] = {nullptr, nullptr, nullptr};  // per-step flags, one byte per face
+    float* prim = nullptr;                  // the step's rho, p, u, v, w (FP32 planes) for the flags
     unsigned long long faces = 0;           // faces evaluated since creation (host count)
     int sms = 148;                          // multiprocessors of the context's device
     bool has_weights = false;
 };
 
-ns_status sensor_create(SensorState** out, const Box&, const FaceBox* fb, cudaStream_t s) {
+ns_status sensor_create(SensorState** out, const Box& b, const FaceBox* fb, cudaStream_t s) {
     *out = nullptr;
     SensorState* st = new (std::nothrow) SensorState();
     if (!st) return NS_ERR_OOM;
     bool ok = cudaMalloc(&st->w, SP * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&st->flagged, sizeof(unsigned long long)) == cudaSuccess;
     for (int d = 0; d < 3 && ok; d++) ok = cudaMalloc(&st->mask[d], (size_t)fb[d].fstride) == cudaSuccess;
+    ok = ok && cudaMalloc(&st->prim, (size_t)5 * b.nx * b.ny * b.nz * sizeof(float)) == cudaSuccess;
     int dev = 0;
     if (ok && cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&st->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -782,6 +800,7 @@ void sensor_destroy(SensorState* st) {
     cudaFree(st->w);
     cudaFree(st->flagged);
     for (int d = 0; d < 3; d++) cudaFree(st->mask[d]);
+    cudaFree(st->prim);
     delete st;
 }
 
@@ -820,9 +839,13 @@ ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box
     const long long tiles = (long long)((fb.n2 + 31) / 32) * ((fb.n1 + 3) / 4) * fb.n0;
     const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
     const dim3 blk(32, 4);
-    if (dir == 0) k_sensor_mask<0><<<grid, blk, 0, s>>>(U0, b, c, fb, st->w, thr, st->mask[0], st->flagged);
-    else if (dir == 1) k_sensor_mask<1><<<grid, blk, 0, s>>>(U0, b, c, fb, st->w, thr, st->mask[1], st->flagged);
-    else k_sensor_mask<2><<<grid, blk, 0, s>>>(U0, b, c, fb, st->w, thr, st->mask[2], st->flagged);
+    if (dir == 0) {  // the first axis of a step forms the primitive planes for all three
+        k_sensor_prims<<<dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx), blk, 0, s>>>(U0, b, c, st->prim);
+        if (launches) (*launches)++;
+    }
+    if (dir == 0) k_sensor_mask<0><<<grid, blk, 0, s>>>(st->prim, b, c, fb, st->w, thr, st->mask[0], st->flagged);
+    else if (dir == 1) k_sensor_mask<1><<<grid, blk, 0, s>>>(st->prim, b, c, fb, st->w, thr, st->mask[1], st->flagged);
+    else k_sensor_mask<2><<<grid, blk, 0, s>>>(st->prim, b, c, fb, st->w, thr, st->mask[2], st->flagged);
     st->faces += (unsigned long long)fb.n0 * fb.n1 * fb.n2;
     if (launches) (*launches)++;
     return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;

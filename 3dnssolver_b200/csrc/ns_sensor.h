@@ -18,7 +18,9 @@ ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const doub
                            const Consts& c, double threshold, bool borges, void* F,
                            const FaceBox& fb, cudaStream_t s, long long* launches);
 // Per-step flags along axis dir for the fused stage kernel: the network on every
-// face of the step's start state U0, one byte per face (FaceBox order).
+// face of the step's start state U0, one byte per face (FaceBox order).  The
+// call for dir 0 (always the first of a step) also forms the FP32 primitive
+// planes the three axes read.
 ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box& b, const Consts& c,
                            double threshold, const FaceBox& fb, cudaStream_t s, long long* launches);
 const unsigned char* sensor_mask(const SensorState* st, int dir);
