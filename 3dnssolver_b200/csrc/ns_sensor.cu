@@ -708,20 +708,26 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ p
     mlp_load(m, w, false);  // once per block: the grid strides over 32 x 4 tiles of faces
     __syncthreads();
     const float gamma = float(c.gamma);
-    const int t2 = (fb.n2 + 31) / 32, t1 = (fb.n1 + 3) / 4;
-    const long long tiles = (long long)t2 * t1 * fb.n0;
+    // tile t = (aa, tile of 4 rows, tile of 32 columns); the host keeps the
+    // tile count below 2^31
+    const unsigned t2 = (fb.n2 + 31) / 32, t1 = (fb.n1 + 3) / 4, t12 = t2 * t1;
+    const unsigned tiles = t12 * (unsigned)fb.n0;
+    const long long n = (long long)b.nx * b.ny * b.nz;
     __nv_bfloat16* X = Xs[warp];
+    // feature columns 24..39 stay zero (K runs to 32; 21..23 are rewritten per tile)
+#pragma unroll
+    for (int e = 24; e < XS; e++) X[lane * XS + e] = __float2bfloat16(0.f);
     unsigned long long nfire = 0;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int kk = (int)(t % t2) * 32 + lane;
-        const int bb = (int)((t / t2) % t1) * 4 + warp;
-        const int aa = (int)(t / ((long long)t2 * t1));
+    for (unsigned t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const unsigned aa_ = t / t12, r = t - aa_ * t12, b1 = r / t2;
+        const int kk = (int)(r - b1 * t2) * 32 + lane;
+        const int bb = (int)b1 * 4 + warp;
+        const int aa = (int)aa_;
         const bool live = kk < fb.n2 && bb < fb.n1;
-        float feat[SF];
+        float feat[24];
         if (live) {
             // face aa lies between cells aa-1 and aa along DIR: stencil aa-3..aa+2;
             // rho, p and u_n in FP32 from the step's primitive planes
-            const long long n = (long long)b.nx * b.ny * b.nz;
             float rho[6], p[6], un[6];
 #pragma unroll
             for (int s = 0; s < 6; s++) {
@@ -739,9 +745,19 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ p
 #pragma unroll
             for (int e = 0; e < SF; e++) feat[e] = 0.f;
         }
+        feat[21] = feat[22] = feat[23] = 0.f;
         __syncwarp();  // the previous tile's fragments are read
+        // three 16-byte stores per row (row stride 80 B: conflict-free per quarter warp)
+        uint4* row = reinterpret_cast<uint4*>(X + lane * XS);
 #pragma unroll
-        for (int e = 0; e < XS; e++) X[lane * XS + e] = __float2bfloat16(e < SF ? feat[e] : 0.f);
+        for (int v = 0; v < 3; v++) {
+            __nv_bfloat162 h0 = __floats2bfloat162_rn(feat[8 * v + 0], feat[8 * v + 1]);
+            __nv_bfloat162 h1 = __floats2bfloat162_rn(feat[8 * v + 2], feat[8 * v + 3]);
+            __nv_bfloat162 h2 = __floats2bfloat162_rn(feat[8 * v + 4], feat[8 * v + 5]);
+            __nv_bfloat162 h3 = __floats2bfloat162_rn(feat[8 * v + 6], feat[8 * v + 7]);
+            row[v] = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
+                                *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
+        }
         __syncwarp();
         float lgs[2][2];
         mlp_logits_fast(m, X, lgs);
@@ -837,6 +853,7 @@ ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box
                            double threshold, const FaceBox& fb, cudaStream_t s, long long* launches) {
     const float thr = (float)std::log(threshold / (1.0 - threshold));
     const long long tiles = (long long)((fb.n2 + 31) / 32) * ((fb.n1 + 3) / 4) * fb.n0;
+    if (tiles >= (1ll << 31)) return NS_ERR_UNSUPPORTED;
     const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
     const dim3 blk(32, 4);
     if (dir == 0) {  // the first axis of a step forms the primitive planes for all three
