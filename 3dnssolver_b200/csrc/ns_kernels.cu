@@ -488,8 +488,11 @@ __global__ void __launch_bounds__(128, NS_UPDATE_MINB) k_update(const double* __
 // viscous terms) overlap the x-faces' FP64 work.  U_out is a second buffer:
 // other threads still read U's x-neighbours for their stencils.
 
+// Cells a thread marches: 24 ran 3% faster than 32 at 256^3 (more, shorter
+// blocks balance the SMs better; the extra x-face per block costs less), 20
+// the same as 24, 43 and 52 slower.
 #ifndef NS_XMARCH_L
-#define NS_XMARCH_L 32
+#define NS_XMARCH_L 24
 #endif
 //
 // LAST (third stage): the next step's start as well -- W = prim(U_out) for its
