@@ -241,7 +241,7 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullp
             launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
                              phys(ctx), fp32(ctx), ctx->W, U, ctx->box, ctx->c, ctx->F[d],
                              ctx->fb[d], ctx->stream, w_only);
-            NS_TRY(check_launch(ctx, 1));
+            NS_TRY(check_launch(ctx, d > 0 ? 2 : 1));  // y and z: the face grid and its last plane
         }
         prof_mark(ctx, NS_PROF_FACE_X + d);
     }

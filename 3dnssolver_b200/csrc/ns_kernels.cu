@@ -223,14 +223,10 @@ struct FaceMinBlocks {
 
 // WONLY (time steps, where W = prim(U)): the stencil reads W only and forms U =
 // cons(W), half the loads; operator calls read the caller's U as given.
-template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY = false>
-__global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
-    k_face_flux(const double* __restrict__ W, const double* __restrict__ U, Box b, Consts c,
-                TF* __restrict__ F, FaceBox fb) {
-    int kk = blockIdx.x * 32 + threadIdx.x;
-    int bb = blockIdx.y * 4 + threadIdx.y;
-    int aa = blockIdx.z;
-    if (kk >= fb.n2 || bb >= fb.n1) return;
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY>
+__device__ __forceinline__ void face_at(const double* __restrict__ W, const double* __restrict__ U,
+                                        const Box& b, const Consts& c, TF* __restrict__ F,
+                                        const FaceBox& fb, int aa, int bb, int kk) {
     long long step;
     long long o0 = face_origin<DIR>(b, aa, bb, kk, step);
     T fL[5][5], fR[5][5], wa[5];
@@ -253,6 +249,34 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
     long long fo = fb.at(aa, bb, kk);
 #pragma unroll
     for (int q = 0; q < 5; q++) F[q * fb.fstride + fo] = TF(out[q]);
+}
+
+// Faces of one (i, j) tile row of 32 k-faces per warp, 4 rows per block.  Along
+// y and z the last face plane (j = ny, k = nz) is left to k_face_flux_tail: as
+// a 33rd k-face or a 4th-of-4 row it would occupy a whole block for one live
+// lane or warp per block.
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY = false>
+__global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
+    k_face_flux(const double* __restrict__ W, const double* __restrict__ U, Box b, Consts c,
+                TF* __restrict__ F, FaceBox fb) {
+    int kk = blockIdx.x * 32 + threadIdx.x;
+    int bb = blockIdx.y * 4 + threadIdx.y;
+    int aa = blockIdx.z;
+    if (kk >= fb.n2 - (DIR == 2) || bb >= fb.n1 - (DIR == 1)) return;
+    face_at<DIR, CHAR, BORGES, PHYS, T, TF, WONLY>(W, U, b, c, F, fb, aa, bb, kk);
+}
+
+// The last face plane along y (j = ny, threads along k) or z (k = nz, threads
+// along j), one face per thread.
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY = false>
+__global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
+    k_face_flux_tail(const double* __restrict__ W, const double* __restrict__ U, Box b, Consts c,
+                     TF* __restrict__ F, FaceBox fb) {
+    static_assert(DIR > 0, "x-faces have no tail plane");
+    const int r = blockIdx.x * 128 + threadIdx.x, aa = blockIdx.y;
+    if (r >= (DIR == 1 ? fb.n2 : fb.n1)) return;
+    const int bb = DIR == 1 ? fb.n1 - 1 : r, kk = DIR == 1 ? r : fb.n2 - 1;
+    face_at<DIR, CHAR, BORGES, PHYS, T, TF, WONLY>(W, U, b, c, F, fb, aa, bb, kk);
 }
 
 // ---------------------------------------------------------------------------
@@ -747,14 +771,18 @@ void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaS
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
 static void face_one(const double* W, const double* U, const Box& b, const Consts& c, void* F,
                      const FaceBox& fb, cudaStream_t s, bool w_only) {
-    dim3 grid((fb.n2 + 31) / 32, (fb.n1 + 3) / 4, fb.n0);
+    const dim3 grid((fb.n2 - (DIR == 2) + 31) / 32, (fb.n1 - (DIR == 1) + 3) / 4, fb.n0);
+    const dim3 tail(((DIR == 1 ? fb.n2 : fb.n1) + 127) / 128, fb.n0);
     if constexpr (sizeof(T) == 8 && DIR > 0) {
         if (w_only) {
             k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF, true><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
+            k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF, true><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb);
             return;
         }
     }
     k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
+    if constexpr (DIR > 0)
+        k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb);
 }
 
 template <int DIR, typename T, typename TF>
