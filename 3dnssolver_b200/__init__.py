@@ -295,7 +295,7 @@ class Solver:
         return sum(n[:3 if p.dim == 3 else 2])
 
     PROFILE_CLASSES = ("step_begin", "fill_prim", "face_x", "face_y", "face_z", "update",
-                       "stage_fused", "sensor", "xface_update")
+                       "stage_fused", "sensor", "xface_update", "viscous")
 
     def profile_step(self):
         """One device-resident step with events between kernels: {kernel class: ms}."""

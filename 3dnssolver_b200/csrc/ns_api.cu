@@ -402,6 +402,14 @@ static ns_status do_step(ns_ctx* ctx) {
         prof_mark(ctx, NS_PROF_FILL);
         NS_TRY(faces(ctx, 1, in[st], true));  // W = prim(U) here: the stencils read W only
         UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
+        if (a.viscous) {  // into the x-face array, which the x-march leaves unused
+            a.V = (const double*)ctx->F[0];
+            a.vs = ctx->fb[0].fstride;
+            launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
+                           ctx->fb[0].fstride, s);
+            NS_TRY(check_launch(ctx, 1));
+            prof_mark(ctx, NS_PROF_VISCOUS);
+        }
         a.U = in[st];
         a.Unext = out[st];
         a.Wnext = ctx->W2;

@@ -505,6 +505,27 @@ __global__ void __launch_bounds__(128, NS_UPDATE_MINB) k_update(const double* __
 }
 
 // ---------------------------------------------------------------------------
+// Viscous terms of every interior cell (residual components 1..4, component 0
+// is zero) into V: plane q-1 of stride vs, cell ((i ny + j) nz + k).  A
+// stencil kernel of its own at full occupancy: inside the x-march its loads sat
+// on the latency path of a 12-warp-per-SM kernel (0.75 ms of 2.47 ms per stage
+// at 256^3, CD-2).
+template <int H, bool PHYS>
+__global__ void __launch_bounds__(128) k_viscous(const double* __restrict__ W, Box b, Consts c,
+                                                 double* __restrict__ V, long long vs) {
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, i = blockIdx.z;
+    if (k >= b.nz || j >= b.ny) return;
+    double rv[5] = {0, 0, 0, 0, 0};
+    if constexpr (PHYS)
+        viscous_physical<H, double>(W, b, c, i, j, k, rv);
+    else
+        viscous_reference<H, double>(W, b, c, i, j, k, rv);
+    const long long e = ((long long)i * b.ny + j) * b.nz + k;
+#pragma unroll
+    for (int q = 1; q < 5; q++) V[(q - 1) * vs + e] = rv[q];
+}
+
+// ---------------------------------------------------------------------------
 // FP64 stage, last kernel: x-face fluxes marched along x with the cell update of
 // each cell as soon as both of its x-faces are known (same face and update
 // arithmetic as k_face_flux<0> + k_update).  The x-face array never reaches
@@ -529,14 +550,16 @@ template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
 __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
     k_xface_update(const double* __restrict__ W, const double* __restrict__ U, double* __restrict__ U0,
                    double* __restrict__ Uout, double* __restrict__ Wn,
-                   const double* __restrict__ Fy, const double* __restrict__ Fz, Box b, FaceBox fy,
+                   const double* __restrict__ Fy, const double* __restrict__ Fz,
+                   const double* __restrict__ V, long long vs, Box b, FaceBox fy,
                    FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
                    unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
                    double* __restrict__ clock) {
     __shared__ double fprev[5][128];  // the x-face below the thread's next cell
-    // the update's operands of cell i (U0, U, the two y- and two z-faces), copied
-    // in while the thread computes x-face i+1; each thread reads only its own
-    __shared__ double opnd[30][128];
+    // the update's operands of cell i (U0, U, the two y- and two z-faces, the
+    // viscous terms from k_viscous), copied in while the thread computes x-face
+    // i+1; each thread reads only its own
+    __shared__ double opnd[H > 0 ? 34 : 30][128];
     const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y;
     const int t = threadIdx.y * 32 + threadIdx.x;
     const int x0 = blockIdx.z * NS_XMARCH_L;
@@ -585,6 +608,11 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
                     cp_async8(&opnd[25 + q][t], Fz + q * fz.fstride + fz.at(i, j, k + 1));
                 }
             }
+            if constexpr (H > 0) {
+                const long long e = ((long long)i * b.ny + j) * b.nz + k;
+#pragma unroll
+                for (int q = 0; q < 4; q++) cp_async8(&opnd[30 + q][t], V + q * vs + e);
+            }
             cp_async_commit();
         }
         double f[5];
@@ -605,13 +633,8 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
             if (convz) r[q] += (opnd[25 + q][t] - opnd[20 + q][t]) * c.inv_dz;
         }
         if constexpr (H > 0) {
-            double rv[5] = {0, 0, 0, 0, 0};
-            if constexpr (PHYS)
-                viscous_physical<H, double>(W, b, c, i, j, k, rv);
-            else
-                viscous_reference<H, double>(W, b, c, i, j, k, rv);
 #pragma unroll
-            for (int q = 1; q < 5; q++) r[q] += rv[q];
+            for (int q = 1; q < 5; q++) r[q] += opnd[29 + q][t];
         }
         double un[5], w[5];
 #pragma unroll
@@ -862,11 +885,25 @@ static void xupd_one(const UpdateArgs& a, cudaStream_t s) {
     if (a.slot_next)
         k_xface_update<CHAR, BORGES, PHYS, H, true><<<grid, dim3(32, 4), 0, s>>>(
             a.W, a.U, const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1], (const double*)a.F[2],
-            a.b, a.fb[1], a.fb[2], a.c, a.flags, a.slot, a.slot_next, a.m1, a.m2, a.mc, a.clock);
+            a.V, a.vs, a.b, a.fb[1], a.fb[2], a.c, a.flags, a.slot, a.slot_next, a.m1, a.m2, a.mc, a.clock);
     else
         k_xface_update<CHAR, BORGES, PHYS, H, false><<<grid, dim3(32, 4), 0, s>>>(
             a.W, a.U, const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1], (const double*)a.F[2],
-            a.b, a.fb[1], a.fb[2], a.c, a.flags, a.slot, nullptr, a.m1, a.m2, a.mc, a.clock);
+            a.V, a.vs, a.b, a.fb[1], a.fb[2], a.c, a.flags, a.slot, nullptr, a.m1, a.m2, a.mc, a.clock);
+}
+
+template <int H, bool PHYS>
+static void visc_one(const double* W, const Box& b, const Consts& c, double* V, long long vs, cudaStream_t s) {
+    k_viscous<H, PHYS><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, V, vs);
+}
+
+void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
+                    long long vs, cudaStream_t s) {
+    switch (h) {
+        case 1: if (phys) visc_one<1, true>(W, b, c, V, vs, s); else visc_one<1, false>(W, b, c, V, vs, s); break;
+        case 2: if (phys) visc_one<2, true>(W, b, c, V, vs, s); else visc_one<2, false>(W, b, c, V, vs, s); break;
+        default: if (phys) visc_one<3, true>(W, b, c, V, vs, s); else visc_one<3, false>(W, b, c, V, vs, s); break;
+    }
 }
 
 template <bool CHAR, bool BORGES, bool PHYS>

@@ -31,6 +31,8 @@ struct UpdateArgs {
     double* Wnext;                   // launch_xface_update: the next stage's W (interior)
     unsigned long long* slot_next;   // launch_xface_update, third stage: the next step's CFL
                                      // minimum (U0 then receives the next step's start)
+    const double* V;                 // launch_xface_update with viscous terms: launch_viscous's output
+    long long vs;                    // its plane stride
 };
 
 // per-face flags of the learned sensor (1 = characteristic-wise), FaceBox order
@@ -79,6 +81,10 @@ void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, cons
 void launch_update(const UpdateArgs& a, cudaStream_t s);
 // FP64 MODE_STAGE: x-faces + update in one march, U_out = a.Unext (a.F[0] unused)
 void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s);
+// viscous terms (components 1..4) of every interior cell into V (plane stride
+// vs >= nx ny nz), half-width h = order/2 of the centered scheme
+void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
+                    long long vs, cudaStream_t s);
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s);
 void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s);
 void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* acc, cudaStream_t s);

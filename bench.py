@@ -270,10 +270,13 @@ def rooflines(form, prof, n, peaks, fma):
            # per-step sensor flags: U0 read once per axis, one byte per face written
            "sensor": 3 * (cells * 40 + faces),
            # x-faces + update: W and U (x stencils), the y- and z-face fluxes and U0
-           # read, U_out and the next stage's W written
-           "xface_update": cells * 280}
+           # read, U_out and the next stage's W written (+ the 4 viscous terms read)
+           "xface_update": cells * 280,
+           # viscous terms: W (rho, p, u, v) read, 4 doubles written per cell
+           "viscous": cells * 64}
     kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})",
-             "sensor": f"k_sensor_mask ({form})", "xface_update": f"k_xface_update ({form})"}.get(
+             "sensor": f"k_sensor_mask ({form})", "xface_update": f"k_xface_update ({form})",
+             "viscous": f"k_viscous ({form})"}.get(
         dom, f"k_face_flux ({dom}, {form})" if dom.startswith("face") else dom)
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9

@@ -163,10 +163,11 @@ NS_API ns_status ns_synchronize(ns_ctx* ctx);
 NS_API ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
 /* Kernel classes timed by ns_profile_step (NS_PROF_SENSOR: the per-step
  * sensor flags of the fused FP32 form; NS_PROF_XFACE_UPDATE: the FP64 x-faces
- * marched together with the cell update) */
+ * marched together with the cell update; NS_PROF_VISCOUS: the FP64 step's
+ * viscous terms) */
 enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FACE_Y = 3,
        NS_PROF_FACE_Z = 4, NS_PROF_UPDATE = 5, NS_PROF_STAGE_FUSED = 6, NS_PROF_SENSOR = 7,
-       NS_PROF_XFACE_UPDATE = 8, NS_PROF_N = 9 };
+       NS_PROF_XFACE_UPDATE = 8, NS_PROF_VISCOUS = 9, NS_PROF_N = 10 };
 /* Runs one time step of the device-resident state with CUDA events recorded
  * between its kernels on the context's stream; ms[c] receives the device time
  * of kernel class c summed over the step, for c < n (n >= 7; classes at or
