@@ -329,27 +329,30 @@ __device__ __forceinline__ void viscous_reference(const double* __restrict__ W, 
 #pragma unroll
         for (int s = 0; s <= 2 * H; s++) {
             if (s == H) continue;
+            // The loads run unconditionally from the wrapped (always valid) row or
+            // column, so that they issue together; a term outside a non-periodic
+            // axis is then dropped by a select.
             // d/dy of (d/dx W) at row j+s-H
-            int jj = j + s - H;
-            if ((jj >= 0 && jj < b.ny) || c.periodic[1]) {
-                int jw = fold(jj, b.ny, 1);
-                long long ob = b.at(i + NG, jw + NG, k + NG);
+            const int jj = j + s - H;
+            {
+                const int jw = fold(jj, b.ny, 1);
+                const long long ob = b.at(i + NG, jw + NG, k + NG);
                 TV dx = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * H; t++)
                     if (t != H) dx += TV(W[q * fs + ob + (t - H) * sx]) * cx1[t];
-                sxy += dx * cy1[s];
+                if ((jj >= 0 && jj < b.ny) || c.periodic[1]) sxy += dx * cy1[s];
             }
             // d/dx of (d/dy W) at column i+s-H
-            int ii = i + s - H;
-            if ((ii >= 0 && ii < b.nx) || c.periodic[0]) {
-                int iw = fold(ii, b.nx, 1);
-                long long ob = b.at(iw + NG, j + NG, k + NG);
+            const int ii = i + s - H;
+            {
+                const int iw = fold(ii, b.nx, 1);
+                const long long ob = b.at(iw + NG, j + NG, k + NG);
                 TV dy = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * H; t++)
                     if (t != H) dy += TV(W[q * fs + ob + (t - H) * sy]) * cy1[t];
-                syx += dy * cx1[s];
+                if ((ii >= 0 && ii < b.nx) || c.periodic[0]) syx += dy * cx1[s];
             }
         }
         Dxy[v] = sxy; Dyx[v] = syx;
