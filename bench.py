@@ -228,9 +228,12 @@ COMPUTE_PER_UNIT = {
     ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
     ("fp64_char", "update"): (316, 205, "fp64", "cell"),
     ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
-    # x-faces marched with the update (first two stages; measured per cell)
-    ("fp64_char", "xface_update"): (1630, 1147, "fp64", "cell"),
+    # x-faces marched with the update (second stage; measured per cell)
+    ("fp64_char", "xface_update"): (1505, 1083, "fp64", "cell"),
     ("fp64_comp", "xface_update"): (1286, 923, "fp64", "cell"),
+    # viscous terms, CD-2 reference semantics (measured per cell)
+    ("fp64_char", "viscous"): (222, 135, "fp64", "cell"),
+    ("fp64_comp", "viscous"): (222, 135, "fp64", "cell"),
     ("fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
     ("fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
 }
@@ -240,7 +243,8 @@ TRAFFIC_PER_UNIT = {
     ("fp64_char", "face_x"): 120.4, ("fp64_char", "face_y"): 118.6, ("fp64_char", "face_z"): 113.6,
     ("fp64_comp", "face_x"): 119.7, ("fp64_comp", "face_y"): 118.7, ("fp64_comp", "face_z"): 113.3,
     ("fp64_char", "update"): 283.7, ("fp64_comp", "update"): 283.7,
-    ("fp64_char", "xface_update"): 311.9, ("fp64_comp", "xface_update"): 306.9,
+    ("fp64_char", "xface_update"): 332.7, ("fp64_comp", "xface_update"): 306.9,
+    ("fp64_char", "viscous"): 51.2, ("fp64_comp", "viscous"): 51.2,
 }
 
 
@@ -271,7 +275,7 @@ def rooflines(form, prof, n, peaks, fma):
            "sensor": 3 * (cells * 40 + faces),
            # x-faces + update: W and U (x stencils), the y- and z-face fluxes and U0
            # read, U_out and the next stage's W written (+ the 4 viscous terms read)
-           "xface_update": cells * 280,
+           "xface_update": cells * 312,
            # viscous terms: W (rho, p, u, v) read, 4 doubles written per cell
            "viscous": cells * 64}
     kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})",
