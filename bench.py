@@ -230,7 +230,7 @@ COMPUTE_PER_UNIT = {
     ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
     # x-faces marched with the update (second stage; measured per cell)
     ("fp64_char", "xface_update"): (1505, 1083, "fp64", "cell"),
-    ("fp64_comp", "xface_update"): (1286, 923, "fp64", "cell"),
+    ("fp64_comp", "xface_update"): (1155, 856, "fp64", "cell"),
     # viscous terms, CD-2 reference semantics (measured per cell)
     ("fp64_char", "viscous"): (222, 135, "fp64", "cell"),
     ("fp64_comp", "viscous"): (222, 135, "fp64", "cell"),
@@ -243,7 +243,7 @@ TRAFFIC_PER_UNIT = {
     ("fp64_char", "face_x"): 120.4, ("fp64_char", "face_y"): 118.6, ("fp64_char", "face_z"): 113.6,
     ("fp64_comp", "face_x"): 119.7, ("fp64_comp", "face_y"): 118.7, ("fp64_comp", "face_z"): 113.3,
     ("fp64_char", "update"): 283.7, ("fp64_comp", "update"): 283.7,
-    ("fp64_char", "xface_update"): 332.7, ("fp64_comp", "xface_update"): 306.9,
+    ("fp64_char", "xface_update"): 332.7, ("fp64_comp", "xface_update"): 330.3,
     ("fp64_char", "viscous"): 51.2, ("fp64_comp", "viscous"): 51.2,
 }
 
