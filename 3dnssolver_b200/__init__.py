@@ -21,8 +21,7 @@ from .abi import (BC_NEUMANN, BC_PERIODIC, CONV_NONE, CONV_WENO5, CONV_WENO5_CHA
                   NsParams, halo_shape, make_params)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-# NS_B200_LIB selects another build of the same library (e.g. a tuning variant)
-LIB_PATH = os.environ.get("NS_B200_LIB") or os.path.join(HERE, "lib", "libns_b200.so")
+LIB_PATH = os.path.join(HERE, "lib", "libns_b200.so")
 
 __all__ = ["Solver", "NsError", "make_params", "halo_shape", "load_library", "abi"]
 
@@ -94,6 +93,18 @@ def _check(status, what):
     if status != 0:
         msg = load_library().ns_last_error_string().decode(errors="replace")
         raise NsError(status, f"{what}: {msg}")
+
+
+def check_host_array(a, shape, writable=False):
+    """Host arrays must be C-contiguous float64 of the reference layout's shape: the C ABI
+    takes plain pointers, so an undersized or strided buffer is refused here, on the host."""
+    if not isinstance(a, np.ndarray) or a.shape != tuple(shape) or a.dtype != np.float64 \
+            or not a.flags["C_CONTIGUOUS"]:
+        got = (getattr(a, "shape", None), getattr(a, "dtype", type(a).__name__))
+        raise ValueError(f"expected a C-contiguous float64 array of shape {tuple(shape)}, got {got}")
+    if writable and not a.flags["WRITEABLE"]:
+        raise ValueError("array must be writable")
+    return a
 
 
 def _dptr(a):
@@ -192,11 +203,7 @@ class Solver:
 
     # -- helpers ----------------------------------------------------------
     def _arr(self, a, writable=False):
-        if a.shape != self.shape or a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
-            raise ValueError(f"expected a C-contiguous float64 array of shape {self.shape}")
-        if writable and not a.flags["WRITEABLE"]:
-            raise ValueError("array must be writable")
-        return a
+        return check_host_array(a, self.shape, writable)
 
     def new_array(self):
         return np.zeros(self.shape, dtype=np.float64)

@@ -50,7 +50,8 @@ class NsParams(ctypes.Structure):
         ("semantics", ctypes.c_int),
         ("sensor", ctypes.c_int),
         ("sensor_threshold", ctypes.c_double),
-        ("reserved", ctypes.c_int * 8),
+        ("check_finite", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
     ]
 
 
@@ -75,7 +76,8 @@ class NsDiagnostics(ctypes.Structure):
 def make_params(nx, ny, nz, *, dim=3, L=(1.0, 1.0, 1.0), mu=1e-3, Pr=0.72, gamma=1.4, cfl=0.5,
                 convection=CONV_WENO5, weights=WEIGHTS_SHU, diffusion=DIFF_CENTERED,
                 diffusion_order=2, bc=(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC),
-                precision=PREC_FP64, semantics=SEM_REFERENCE, sensor=0, sensor_threshold=0.5):
+                precision=PREC_FP64, semantics=SEM_REFERENCE, sensor=0, sensor_threshold=0.5,
+                check_finite=0):
     p = NsParams()
     p.dim, p.nx, p.ny, p.nz = dim, nx, ny, nz
     p.Lx, p.Ly, p.Lz = L
@@ -86,6 +88,7 @@ def make_params(nx, ny, nz, *, dim=3, L=(1.0, 1.0, 1.0), mu=1e-3, Pr=0.72, gamma
         p.bc[a] = bc[a]
     p.precision, p.semantics = precision, semantics
     p.sensor, p.sensor_threshold = sensor, sensor_threshold
+    p.check_finite = check_finite
     return p
 
 

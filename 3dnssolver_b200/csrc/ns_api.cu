@@ -7,7 +7,6 @@
 #include <cstdio>
 #include <cstring>
 #include <utility>
-#include <mutex>
 #include <new>
 #include <string>
 
@@ -112,13 +111,13 @@ static ns_status validate(const ns_params* p) {
         return fail(NS_ERR_INVALID_ARG, "unknown precision %d", p->precision);
     if (p->semantics != NS_SEM_REFERENCE && p->semantics != NS_SEM_PHYSICAL)
         return fail(NS_ERR_INVALID_ARG, "unknown semantics %d", p->semantics);
+    if (p->check_finite != 0 && p->check_finite != 1)
+        return fail(NS_ERR_INVALID_ARG, "check_finite must be 0 or 1 (got %d)", p->check_finite);
     if (p->sensor) {
         if (p->convection != NS_CONV_WENO5_CHAR)
             return fail(NS_ERR_INVALID_ARG, "the sensor gates the characteristic scheme: convection must be NS_CONV_WENO5_CHAR");
         if (p->precision != NS_PREC_FP32)
             return fail(NS_ERR_INVALID_ARG, "the sensor-gated form runs in NS_PREC_FP32");
-        if (p->semantics != NS_SEM_REFERENCE)
-            return fail(NS_ERR_INVALID_ARG, "the sensor-gated form follows the reference semantics");
         if (!(p->sensor_threshold > 0.0 && p->sensor_threshold < 1.0))
             return fail(NS_ERR_INVALID_ARG, "sensor_threshold must lie in (0,1)");
     }
@@ -233,7 +232,7 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullp
     for (int d = first_dir; d < nd; d++) {
         if (p.sensor) {
             if (sensor_face_flux(ctx->sensor, d, ctx->W, ctx->U, ctx->box, ctx->c, p.sensor_threshold,
-                                 p.weights == NS_WEIGHTS_BORGES, ctx->F[d], ctx->fb[d], ctx->stream,
+                                 p.weights == NS_WEIGHTS_BORGES, phys(ctx), ctx->F[d], ctx->fb[d], ctx->stream,
                                  &ctx->launches) != NS_OK)
                 return fail(NS_ERR_CUDA, "gated face kernel launch failed: %s",
                             cudaGetErrorString(cudaGetLastError()));
@@ -279,7 +278,7 @@ static ns_status do_step_fused(ns_ctx* ctx) {
     if (!ctx->fused_ready) {
         // dt from W at the step start (set_dt) and U0 = cons(W) (time_scheme.cpp:124-126)
         NS_CUDA(cudaMemsetAsync(cur, 0xFF, sizeof(unsigned long long), s));
-        launch_step_begin(!ctx->w_valid, false, ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s);
+        launch_step_begin(!ctx->w_valid, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s);
         NS_TRY(check_launch(ctx, 1));
         prof_mark(ctx, NS_PROF_STEP_BEGIN);
     }
@@ -294,6 +293,7 @@ static ns_status do_step_fused(ns_ctx* ctx) {
     a.fp32 = fp32(ctx);
     a.chr = p.convection == NS_CONV_WENO5_CHAR;
     a.borges = p.weights == NS_WEIGHTS_BORGES;
+    a.phys = phys(ctx);
     a.U0 = ctx->U0;
     a.slot = cur;
     a.slot_next = nxt;
@@ -450,6 +450,26 @@ static ns_status finalize_w(ns_ctx* ctx) {
     return NS_OK;
 }
 
+// params.check_finite: counts the interior cells of the current state that hold
+// NaN/Inf or a non-positive density or pressure (waits for the stream)
+static ns_status check_state(ns_ctx* ctx) {
+    if (!ctx->p.check_finite || (!ctx->w_valid && !ctx->u_valid)) return NS_OK;
+    cudaStream_t s = ctx->stream;
+    unsigned long long* cnt = ctx->slot + 3;
+    NS_CUDA(cudaMemsetAsync(cnt, 0, sizeof *cnt, s));
+    if (ctx->u_valid) launch_check_state(ctx->U, false, ctx->box, ctx->c, cnt, s);
+    else launch_check_state(ctx->W, true, ctx->box, ctx->c, cnt, s);
+    NS_TRY(check_launch(ctx, 1));
+    unsigned long long n = 0;
+    NS_CUDA(cudaMemcpyAsync(&n, cnt, sizeof n, cudaMemcpyDeviceToHost, s));
+    NS_CUDA(cudaStreamSynchronize(s));
+    if (n)
+        return fail(NS_ERR_NONFINITE,
+                    "%llu interior cells hold NaN/Inf or a non-positive density or pressure after %lld steps",
+                    n, ctx->steps);
+    return NS_OK;
+}
+
 static double slot_dt(unsigned long long bits, double cfl) {
     double v;
     memcpy(&v, &bits, sizeof v);
@@ -560,12 +580,12 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
         for (int d = 0; d < (p->dim == 3 ? 3 : 2); d++)
             A(&ctx->F[d], (size_t)ctx->fb[d].fstride * NS_NQ * fe);
     A((void**)&ctx->slot, 4 * sizeof(unsigned long long));
-    // The fused stage kernel serves the FP32 form of the reference semantics.  In
-    // FP64 its shared-memory box (one 198 KB block per SM) leaves nothing to
-    // overlap the load and compute phases with, and the FP64-pipe-bound face
-    // kernels of the unfused path run faster (measured on B200 at 256^3:
-    // 2.18 vs 3.06 G cell-updates/s for the characteristic scheme).
-    ctx->fused = (p->semantics == NS_SEM_REFERENCE) && p->precision == NS_PREC_FP32;
+    // The fused stage kernel serves the FP32 form (both semantics).  In FP64 its
+    // shared-memory ring (one 198 KB block per SM) leaves nothing to overlap the
+    // load and compute phases with, and the FP64-pipe-bound face kernels of the
+    // unfused path run faster (measured on B200 at 256^3: 2.18 vs 3.06 G
+    // cell-updates/s for the characteristic scheme).
+    ctx->fused = p->precision == NS_PREC_FP32;
     ctx->xfused = !ctx->fused && p->precision == NS_PREC_FP64 && p->convection != NS_CONV_NONE;
     if (ctx->fused || ctx->xfused) A((void**)&ctx->U2, soa_bytes(ctx->box));
     if (ctx->xfused) A((void**)&ctx->W2, soa_bytes(ctx->box));
@@ -712,7 +732,7 @@ ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
     NS_TRY(download(ctx, ctx->W, W));
     if (U) NS_TRY(download(ctx, ctx->U, U));
     if (dt_out) *dt_out = clk[0];
-    return NS_OK;
+    return check_state(ctx);
 }
 
 ns_status ns_advance(ns_ctx* ctx, int nsteps) {
@@ -720,7 +740,7 @@ ns_status ns_advance(ns_ctx* ctx, int nsteps) {
     if (nsteps < 0) return fail(NS_ERR_INVALID_ARG, "nsteps must be >= 0");
     if (!ctx->w_valid && !ctx->u_valid) return fail(NS_ERR_INVALID_ARG, "no state has been uploaded");
     for (int n = 0; n < nsteps; n++) NS_TRY(do_step(ctx));
-    return NS_OK;
+    return check_state(ctx);
 }
 
 ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time) {
@@ -736,7 +756,7 @@ ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time) {
 ns_status ns_synchronize(ns_ctx* ctx) {
     if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
     NS_CUDA(cudaStreamSynchronize(ctx->stream));
-    return NS_OK;
+    return check_state(ctx);
 }
 
 ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out) {
@@ -871,7 +891,7 @@ ns_status ns_sensor_harvest(ns_ctx* ctx, float* feat, float* label, long long ca
     ctx->halos_stale = false;
     long long base = 0;
     for (int d = 0; d < nd; d++) {
-        if (sensor_harvest(d, ctx->p.weights == NS_WEIGHTS_BORGES, ctx->W, ctx->U, ctx->box, ctx->c,
+        if (sensor_harvest(d, ctx->p.weights == NS_WEIGHTS_BORGES, phys(ctx), ctx->W, ctx->U, ctx->box, ctx->c,
                            ctx->fb[d], base, rel_threshold, feat, label, s) != NS_OK)
             return fail(NS_ERR_CUDA, "harvest kernel launch failed: %s", cudaGetErrorString(cudaGetLastError()));
         NS_TRY(check_launch(ctx, 1));
@@ -896,8 +916,15 @@ ns_status ns_sensor_harvest(ns_ctx* ctx, float* feat, float* label, long long ca
 // fixed array compiled into the library.
 //
 // Cost and limits: the array takes NS_NOALLOC_SCRATCH_BYTES (32 MiB) on every
-// GPU that loads this library, for the life of the process.  A grid fits when
-// the face fluxes of all convected axes fit in it (FP64: 5 doubles per face;
+// GPU where this library's device code is loaded, for the life of the process.
+// CUDA loads a library's device code onto a device lazily by default (since
+// CUDA 12.2), at the first use of one of its kernels or symbols there, so the
+// array may be reserved by the first call of this entry point on a device; a
+// caller that must not see an out-of-memory failure later makes one call at
+// start-up (or runs with CUDA_MODULE_LOADING=EAGER).  That first call on a
+// device also loads the device code, which is not allowed inside a stream
+// capture: make it before any capture begins.  A grid fits when the face
+// fluxes of all convected axes fit in the array (FP64: 5 doubles per face;
 // about 64^3 cells in 3D); larger grids are rejected with NS_ERR_INVALID_ARG.
 // All calls on a device share the array, so calls whose kernels overlap on
 // that GPU (different streams, or several host threads) race and corrupt each
@@ -906,32 +933,25 @@ ns_status ns_sensor_harvest(ns_ctx* ctx, float* feat, float* label, long long ca
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = NS_NOALLOC_SCRATCH_BYTES;
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kNoAllocMaxDevices] = {};
-
-// Device address of the scratch array on the current device.  The symbol's
-// host-side name is only a stand-in, so its address is looked up once per
-// device with that device current (the first call on each device).
+// Device address of the scratch array in the current context.  The symbol's
+// host-side name is only a stand-in, so the address is looked up with the
+// target device current, on every call: a cached address would go stale when
+// the context is destroyed (cudaDeviceReset) or when the caller switches to
+// another context on the same device.  The lookup is a host-side table read
+// once the device code is loaded.
 ns_status noalloc_scratch(void** out) {
-    int dev = -1;
-    NS_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kNoAllocMaxDevices)
-        return fail(NS_ERR_UNSUPPORTED, "device ordinal %d is beyond the %d devices supported", dev,
-                    kNoAllocMaxDevices);
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void* ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess || !ptr)
-            return fail(NS_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
-                        cudaGetErrorString(e));
-        g_noalloc_addr[dev] = ptr;
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+        int dev = -1;
+        cudaGetDevice(&dev);
+        return fail(NS_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
+                    cudaGetErrorString(e));
     }
-    *out = g_noalloc_addr[dev];
+    *out = ptr;
     return NS_OK;
 }
 

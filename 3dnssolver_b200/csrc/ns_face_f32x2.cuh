@@ -9,8 +9,11 @@
 //   lane y: fR of cells a+3, a+2, a+1, a, a-1
 // The characteristic projection (Weno5cw::compute_num_flux, weno-5cw.cpp:4-28)
 // is linear, so the left and right columns of the same stencil position are
-// projected together as well.  Reference semantics only (Q1-Q4: alpha = 3,
-// c2 = gamma/(p rho), textbook rows applied to the state order).
+// projected together as well.  PHYS = false: the reference semantics (alpha = 3,
+// c2 = gamma/(p rho), textbook rows applied to the state order,
+// convection_flux.cpp:139,153-171,241); PHYS = true: the physical form (local
+// alpha = max(|q_n| + c) over the 6-cell stencil, c2 = gamma p/rho, rows
+// permuted to the state order).
 #pragma once
 
 #include "ns_face.cuh"
@@ -99,12 +102,15 @@ __device__ __forceinline__ void cell_pair_f32x2(const f2 w[5], float hg, float i
 // Packed stencil of one face: P[q][k] = (fL_q of cell k, fR_q of cell 5-k),
 // cells 0..5 = a-2..a+3, from W at the 6 cells: cells k and 5-k share a lane
 // pair for U = cons(W) and half the Euler flux (division free); Lax-Friedrichs
-// split with alpha = 3.  wa receives the face average of W (cells 2 and 3).
-template <int DIR, bool CHAR>
+// split with alpha = 3 (PHYS: the largest |q_n| + c of the 6 cells, c from one
+// reciprocal square root: sqrt(gamma p/rho) = gamma p rsqrt(gamma p rho)).
+// wa receives the face average of W (cells 2 and 3).
+template <int DIR, bool CHAR, bool PHYS = false>
 __device__ __forceinline__ void stencil_f32x2(const float* const* planes, int c0, int step, int fs,
                                               float gamma, float inv_gm1, f2 P[5][5], float wa[5]) {
     const float hg = 0.5f * gamma * inv_gm1;
     f2 U[3][5], F[3][5];
+    float amax = 0.f;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
         const float* A = planes[k];
@@ -119,32 +125,41 @@ __device__ __forceinline__ void stencil_f32x2(const float* const* planes, int c0
                 for (int q = 0; q < 5; q++) wa[q] = 0.5f * (w[q].x + w[q].y);
             }
         }
+        if constexpr (PHYS) {
+            const f2 gp = mul2(sp2(gamma), w[1]);
+            const f2 gpr = mul2(gp, w[0]);
+            const float cx = gp.x * rsqrtf(gpr.x), cy = gp.y * rsqrtf(gpr.y);
+            amax = fmaxf(amax, fmaxf(fabsf(w[2 + DIR].x) + cx, fabsf(w[2 + DIR].y) + cy));
+        }
         cell_pair_f32x2<DIR>(w, hg, inv_gm1, U[k], F[k]);
     }
-    const f2 lr = make_float2(1.5f, -1.5f);
+    const float ha = PHYS ? 0.5f * amax : 1.5f;
+    const f2 lr = make_float2(ha, -ha);
 #pragma unroll
     for (int q = 0; q < 5; q++) {
 #pragma unroll
         for (int k = 0; k < 3; k++) P[q][k] = fma2(lr, U[k][q], F[k][q]);
         // k = 3, 4: the pairs (2,3) and (1,4) with their lanes swapped
-        P[q][3] = make_float2(fmaf(1.5f, U[2][q].y, F[2][q].y), fmaf(-1.5f, U[2][q].x, F[2][q].x));
-        P[q][4] = make_float2(fmaf(1.5f, U[1][q].y, F[1][q].y), fmaf(-1.5f, U[1][q].x, F[1][q].x));
+        P[q][3] = make_float2(fmaf(ha, U[2][q].y, F[2][q].y), fmaf(-ha, U[2][q].x, F[2][q].x));
+        P[q][4] = make_float2(fmaf(ha, U[1][q].y, F[1][q].y), fmaf(-ha, U[1][q].x, F[1][q].x));
     }
 }
 
-template <int DIR, bool CHAR, bool BORGES>
+template <int DIR, bool CHAR, bool BORGES, bool PHYS = false>
 __device__ __forceinline__ void face_f32x2(const float* const* planes, int c0, int step, int fs, float gamma,
                                            float inv_gm1, float out[5]) {
     f2 P[5][5];
     float wa[5];
-    stencil_f32x2<DIR, CHAR>(planes, c0, step, fs, gamma, inv_gm1, P, wa);
+    stencil_f32x2<DIR, CHAR, PHYS>(planes, c0, step, fs, gamma, inv_gm1, P, wa);
     if constexpr (!CHAR) {
 #pragma unroll
         for (int q = 0; q < 5; q++) out[q] = weno_f32x2<BORGES>(P[q][0], P[q][1], P[q][2], P[q][3], P[q][4]);
         return;
     } else {
-        const Eig<float> e = make_eig<DIR, false, float>(wa, gamma, inv_gm1);
+        const Eig<float> e = make_eig<DIR, PHYS, float>(wa, gamma, inv_gm1);
         using F = Frame<DIR>;
+        // state index of textbook component t (identity for the reference semantics)
+        constexpr int s0 = st<PHYS>(0), s1 = st<PHYS>(1), s2 = st<PHYS>(2), s3 = st<PHYS>(3), s4 = st<PHYS>(4);
         // rows of L (make_eig's scalars); the tangential rows are kept up to
         // their sign (l_sg, m_sg): WENO is odd, so the sign is applied after it
         const f2 v0 = sp2(e.vel[0]), v1 = sp2(e.vel[1]), v2 = sp2(e.vel[2]);
@@ -155,8 +170,8 @@ __device__ __forceinline__ void face_f32x2(const float* const* planes, int c0, i
         f2 C[5][5];
 #pragma unroll
         for (int k = 0; k < 5; k++) {
-            const f2 f0 = P[0][k], fe = P[4][k];
-            const f2 fm[3] = {P[1][k], P[2][k], P[3][k]};
+            const f2 f0 = P[s0][k], fe = P[s4][k];
+            const f2 fm[3] = {P[s1][k], P[s2][k], P[s3][k]};
             f2 g = sub2(fma2(v0, fm[0], fma2(v1, fm[1], mul2(v2, fm[2]))), fe);  // u.fm - fE
             C[1][k] = fma2(nqm, f0, fm[F::m_ax]);                                 // m_sg * row 1
             C[4][k] = fma2(nql, f0, fm[F::l_ax]);                                 // l_sg * row 4
@@ -172,17 +187,18 @@ __device__ __forceinline__ void face_f32x2(const float* const* planes, int c0, i
         ft[4] *= float(F::l_sg);
         // back-projection R ft (textbook rows of R, convection_flux.cpp:153-158)
         const float acc = ft[0] + ft[2] + ft[3];
-        out[0] = acc;
+        out[s0] = acc;
+        constexpr int sm[3] = {s1, s2, s3};
 #pragma unroll
         for (int ax = 0; ax < 3; ax++) {
             float cn = (ax == DIR) ? e.c : 0.f;
             float v = e.vel[ax] * acc - cn * ft[0] + cn * ft[3];
             if (ax == F::m_ax) v += (F::m_sg > 0 ? ft[1] : -ft[1]);
             if (ax == F::l_ax) v += (F::l_sg > 0 ? ft[4] : -ft[4]);
-            out[1 + ax] = v;
+            out[sm[ax]] = v;
         }
-        out[4] = e.H * (ft[0] + ft[3]) + e.qn * e.c * (ft[3] - ft[0]) + e.qm * ft[1] + 0.5f * e.q2 * ft[2] +
-                 e.ql * ft[4];
+        out[s4] = e.H * (ft[0] + ft[3]) + e.qn * e.c * (ft[3] - ft[0]) + e.qm * ft[1] + 0.5f * e.q2 * ft[2] +
+                  e.ql * ft[4];
     }
 }
 

@@ -1,424 +1,11 @@
-// ns_fused.cu -- one kernel per SSP-RK3 stage (reference semantics).
-//
-// A block owns a TY x TZ column of cells and marches along x.  Every plane it
-// touches is loaded once with 3 ghost rows and columns, folding each axis by
-// its boundary condition (periodic wrap or Neumann clamp: the single-GPU form
-// of Domain::apply_boundary_conditions + Communicator::communicate,
-// src/domain.cpp:18-28, src/communicator.cpp:6-143), and kept as W = prim(U)
-// (src/eq_of_state.cpp:61-87) in a shared-memory ring of 7 planes.  For each
-// cell it forms the face fluxes along x (carried from cell to cell in
-// registers), y and z, accumulates (f(+) - f(-))/d in the reference's order
-// (Weno5::compute_residual, weno-5.cpp:39-73), adds the centered viscous terms
-// from the ring, and writes U_out = U0 m1 + U_in m2 + R mc dt
-// (TimeScheme::substep, time_scheme.cpp:72-96).  U_in and U_out are different
-// buffers: neighbouring blocks read U_in's cells as their ghost layers.
-//
-// The third stage also takes the next step's start: W = prim(U_out) for the
-// CFL minimum (time_scheme.cpp:69, 98-136) and U0 = cons(W) (the W -> U
-// round trip of time_scheme.cpp:124), so a step is three launches.
-//
-// The Lax-Friedrichs split uses U = cons(W) of the ring's W; it differs from
-// the stage's U by rounding only.
-#include <cuda_runtime.h>
-
-#include "ns_common.cuh"
-#include "ns_eos.cuh"
-#include "ns_face.cuh"
-#include "ns_face_f32x2.cuh"
-#include "ns_kernels.h"
-#include "ns_viscous.cuh"
+// ns_fused.cu -- dispatch of the fused FP32 stage kernel (ns_fused.cuh) by
+// semantics; the kernels are compiled in ns_fused_ref.cu and ns_fused_phys.cu.
+#include "ns_fused.cuh"
 
 namespace nsb {
 
-constexpr int FT = 256;  // threads per block
-
-// ---------------------------------------------------------------------------
-// A block marches LX cells along x over a TY x TZ column: 2.2 plane loads per
-// cell (a 3D box tile with the same shared memory needed 7.4 and ran 20%
-// slower on B200), x-face fluxes carried in registers, y- and z-faces of the
-// current plane through small shared face buffers.
-
-// TY x TZ = 8 x 32 cells per plane, one per thread.  A 7-row tile (one round
-// per face pass instead of two for the 288 y- and 264 z-faces) measured the
-// same on B200 (+2.6% component-wise, -3% characteristic), so the plane of 8
-// rows stays; NS_MARCH_TY selects it at build time.
-#ifndef NS_MARCH_TY
-#define NS_MARCH_TY 8
-#endif
-//
-// Plane i reads planes i-2..i+3 (x-faces) and i-H..i+H (viscous terms).  With
-// H <= 1 ("lean") the ring holds 6 planes and the y/z face buffers alternate
-// between planes, so a plane needs two block barriers instead of three: the
-// next plane's conversion overwrites plane i-2, whose last reader (the x-faces)
-// finished before this plane's second barrier.
-template <typename T, int H = 1>
-struct MarchTile {
-    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = 32;
-    static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
-    static constexpr bool LEAN = H <= 1;
-    static constexpr int RING = LEAN ? 6 : 7;
-    static constexpr int NBUF = LEAN ? 2 : 1;
-    static constexpr int NFY = (TY + 1) * TZ, NFZ = TY * (TZ + 1);
-    static constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
-    // ring, y/z face buffers, and the FP64 conserved state of the plane in flight
-    static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) +
-                                   (size_t)NBUF * 5 * (NFY + NFZ) * sizeof(T) + (size_t)5 * NP * sizeof(double);
-};
-
-
-// Thread index rotated so that warp w handles items 0..31 of every round of a
-// pass: the partial last round of each pass (plane loads, y-faces, z-faces)
-// then falls to a different warp instead of piling up on warp 0 before the
-// same barrier.
-__device__ __forceinline__ int rotated(int tid, int w) { return (tid + FT - 32 * w) % FT; }
-
-template <int RING>
-__device__ __forceinline__ int ring_slot(int i, int x0) {
-    return (i - x0 + 3) % RING;  // i >= x0 - 3
-}
-
-// one face from a 6-cell stencil in a shared array with stride `step`
-// (GATE: the characteristic-wise form where `fire`, the component-wise elsewhere)
-template <int DIR, bool CHAR, bool BORGES, bool GATE, typename T>
-__device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, T gamma,
-                                           T inv_gm1, bool fire, T out[5]) {
-    if constexpr (sizeof(T) == 4) {
-        if constexpr (GATE) {
-            if (fire)
-                face_f32x2<DIR, true, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
-            else
-                face_f32x2<DIR, false, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
-        } else {
-            face_f32x2<DIR, CHAR, BORGES>(planes, c0, step, fs, gamma, inv_gm1, out);
-        }
-        return;
-    }
-    const T hg = T(0.5) * gamma * inv_gm1;
-    T fL[5][5], fR[5][5], wa[5];
-#pragma unroll
-    for (int s = 0; s < 6; s++) {
-        const T* P = planes[s];
-        int idx = c0 + s * step;
-        T w[5], u[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) w[q] = P[q * fs + idx];
-        u[0] = w[0];
-        u[2] = w[0] * w[2];
-        u[3] = w[0] * w[3];
-        u[4] = w[0] * w[4];
-        u[1] = w[1] * inv_gm1 + T(0.5) * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-        split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
-    }
-    if constexpr (CHAR)
-        face_char<DIR, false, T, BORGES>(fL, fR, wa, gamma, inv_gm1, out);
-    else
-        face_comp<T, BORGES>(fL, fR, out);
-}
-
-
-// centered viscous terms of the cell at plane i, in-plane index cc, from the
-// ring (reference semantics): mixed derivatives differentiate first
-// derivatives that are zero outside the interior along a non-periodic axis
-// (centered_diffusion.cpp:22-24)
-template <int H, typename T, typename PlaneFn>
-__device__ __forceinline__ void march_viscous(PlaneFn plane, int i, int cc, const Consts& c, int nx,
-                                              int ny, int gi, int gj, T r[5]) {
-    using M = MarchTile<T>;
-    const int sy = M::PZ, fs = M::NP;
-    T cx1[2 * H + 1], cy1[2 * H + 1], cxx[2 * H + 1], cyy[2 * H + 1];
-#pragma unroll
-    for (int t = 0; t <= 2 * H; t++) {
-        cx1[t] = T(c.df[3 - H + t] * c.inv_dx);
-        cy1[t] = T(c.df[3 - H + t] * c.inv_dy);
-        cxx[t] = T(c.ddf[3 - H + t] * c.inv_dx * c.inv_dx);
-        cyy[t] = T(c.ddf[3 - H + t] * c.inv_dy * c.inv_dy);
-    }
-    const T* P[2 * H + 1];
-#pragma unroll
-    for (int t = 0; t <= 2 * H; t++) P[t] = plane(i + t - H);
-    T Dx[4], Dy[4], Dxx[4], Dyy[4];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        T a1 = 0, b1 = 0, a2 = 0, b2 = 0;
-#pragma unroll
-        for (int t = 0; t <= 2 * H; t++) {
-            T wx = P[t][q * fs + cc];
-            T wy = P[H][q * fs + cc + (t - H) * sy];
-            if (t != H) { a1 += wx * cx1[t]; b1 += wy * cy1[t]; }
-            a2 += wx * cxx[t];
-            b2 += wx * cyy[t];  // d2/dy2 uses the x-stencil (cd-n.cpp:77)
-        }
-        Dx[q] = a1; Dy[q] = b1; Dxx[q] = a2; Dyy[q] = b2;
-    }
-    T Dxy[2], Dyx[2];
-#pragma unroll
-    for (int v = 0; v < 2; v++) {
-        const int q = 2 + v;
-        T sxy = 0, syx = 0;
-#pragma unroll
-        for (int s = 0; s <= 2 * H; s++) {
-            if (s == H) continue;
-            int jj = gj + s - H;
-            if ((jj >= 0 && jj < ny) || c.periodic[1]) {
-                T dx = 0;
-#pragma unroll
-                for (int t = 0; t <= 2 * H; t++)
-                    if (t != H) dx += P[t][q * fs + cc + (s - H) * sy] * cx1[t];
-                sxy += dx * cy1[s];
-            }
-            int ii = gi + s - H;
-            if ((ii >= 0 && ii < nx) || c.periodic[0]) {
-                T dy = 0;
-#pragma unroll
-                for (int t = 0; t <= 2 * H; t++)
-                    if (t != H) dy += P[s][q * fs + cc + (t - H) * sy] * cy1[t];
-                syx += dy * cx1[s];
-            }
-        }
-        Dxy[v] = sxy; Dyx[v] = syx;
-    }
-    viscous_reference_terms<T>(Dx, Dy, Dxx, Dyy, Dxy, Dyx, P[H][2 * fs + cc], P[H][3 * fs + cc],
-                               P[H][1 * fs + cc], P[H][cc], c, r);
-}
-
-template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool GATE>
-__global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
-    k_stage_march(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
-                  Consts c, int conv_dims, double m1, double m2, double mc,
-                  const unsigned long long* __restrict__ slot, unsigned long long* slot_next,
-                  double* clock, Gate gate) {
-    using M = MarchTile<T, H>;
-    static_assert(M::NFY <= 2 * FT && M::NFZ <= 2 * FT, "a face pass takes at most two rounds");
-    extern __shared__ __align__(16) unsigned char smem[];
-    T* ring = reinterpret_cast<T*>(smem);        // [RING][5][NP]
-    T* FYb = ring + M::RING * 5 * M::NP;         // [NBUF][5][NFY]
-    T* FZb = FYb + M::NBUF * 5 * M::NFY;         // [NBUF][5][NFZ]
-    double* S = reinterpret_cast<double*>(FZb + M::NBUF * 5 * M::NFZ);  // [5][NP] U_in of the plane in flight
-    const int tid = threadIdx.x, ty = tid / M::TZ, tz = tid % M::TZ;
-    const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * M::LX;
-    const int x1 = min(x0 + M::LX, b.nx);
-    const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
-    auto plane = [&](int i) { return ring + ring_slot<M::RING>(i, x0) * 5 * M::NP; };
-    // U_in of plane i at folded positions, into S without waiting (each thread
-    // later converts exactly the elements it copied, so S needs no barrier)
-    auto issue_plane = [&](int i) {
-        const int gi = fold(i, b.nx, c.periodic[0]);
-        for (int e = rotated(tid, 5); e < M::NP; e += FT) {
-            int py = e / M::PZ, pz = e % M::PZ;
-            int gj = fold(j0 - 3 + py, b.ny, c.periodic[1]);
-            int gk = fold(k0 - 3 + pz, b.nz, c.periodic[2]);
-            long long o = b.at(gi + NG, gj + NG, gk + NG);
-#pragma unroll
-            for (int q = 0; q < 5; q++) cp_async8(S + q * M::NP + e, Uin + q * b.fstride + o);
-        }
-        cp_async_commit();
-    };
-    // W = prim(U_in) of the plane in S into plane i's ring slot
-    auto convert_plane = [&](int i) {
-        cp_async_wait_all();
-        T* P = plane(i);
-        for (int e = rotated(tid, 5); e < M::NP; e += FT) {
-            if constexpr (sizeof(T) == 4) {
-                // the FP32 form's W in FP32 arithmetic from the FP64 state
-                float u[5];
-#pragma unroll
-                for (int q = 0; q < 5; q++) u[q] = float(S[q * M::NP + e]);
-                const float ir = __fdividef(1.f, u[0]);
-                const float vx = u[2] * ir, vy = u[3] * ir, vz = u[4] * ir;
-                P[e] = u[0];
-                P[M::NP + e] = float(c.gm1) * (u[1] - 0.5f * u[0] * (vx * vx + vy * vy + vz * vz));
-                P[2 * M::NP + e] = vx;
-                P[3 * M::NP + e] = vy;
-                P[4 * M::NP + e] = vz;
-            } else {
-                double u[5], w[5];
-#pragma unroll
-                for (int q = 0; q < 5; q++) u[q] = S[q * M::NP + e];
-                prim_from_cons(u, c.gm1, w);
-#pragma unroll
-                for (int q = 0; q < 5; q++) P[q * M::NP + e] = T(w[q]);
-            }
-        }
-    };
-    auto load_plane = [&](int i) {
-        issue_plane(i);
-        convert_plane(i);
-    };
-    // x-face of this thread's column between cells i and i+1 (stencil i-2..i+3)
-    const int ccol = (ty + 3) * M::PZ + (tz + 3);
-    auto xface = [&](int i, bool fire, T out[5]) {
-        const T* P[6];
-#pragma unroll
-        for (int s = 0; s < 6; s++) P[s] = plane(i - 2 + s);
-        march_face<0, CHAR, BORGES, GATE, T>(P, ccol, 0, M::NP, gamma, inv_gm1, fire, out);
-    };
-    const int gj = j0 + ty, gk = k0 + tz;
-    const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
-    const bool own = row && gj < b.ny && gk < b.nz;
-    // sensor flags of this thread's faces of plane i (x-face i+1/2, up to two y- and
-    // two z-faces), loaded early and tested only in the face pass; i = x0 - 1 (the
-    // first x-face) can be -1, which has no y- or z-faces
-    unsigned char gx = 0, gy[2] = {0, 0}, gz[2] = {0, 0};
-    auto load_flags = [&](int i) {
-        if constexpr (GATE) {
-            gx = own ? gate.m[0][gate.fb[0].at(i + 1, gj, gk)] : 0;
-#pragma unroll
-            for (int r = 0; r < 2; r++) {
-                int e = rotated(tid, 7) + r * FT;
-                int a = j0 + e / M::TZ, kk = k0 + e % M::TZ;
-                gy[r] = (i >= 0 && e < M::NFY && a <= b.ny && kk < b.nz) ? gate.m[1][gate.fb[1].at(i, a, kk)] : 0;
-                e = rotated(tid, 6) + r * FT;
-                int jj = j0 + e / (M::TZ + 1);
-                a = k0 + e % (M::TZ + 1);
-                gz[r] = (i >= 0 && conv_dims == 3 && e < M::NFZ && jj < b.ny && a <= b.nz)
-                            ? gate.m[2][gate.fb[2].at(i, jj, a)] : 0;
-            }
-        }
-    };
-    for (int i = x0 - 3; i < x0 + 3; i++) load_plane(i);
-    issue_plane(x0 + 3);
-    __syncthreads();
-    T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
-    load_flags(x0 - 1);
-    if (conv_dims > 0 && row) xface(x0 - 1, gx != 0, fxl);
-    if constexpr (M::LEAN) __syncthreads();  // plane x0+3 takes the slot of plane x0-3
-    const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
-    const double m3 = mc * dt;
-    if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | tid) == 0) {
-        clock[0] = dt;
-        clock[1] += dt;
-    }
-    double best = INFINITY;
-    for (int i = x0; i < x1; i++) {
-        load_flags(i);
-        convert_plane(i + 3);
-        __syncthreads();
-        if (i + 1 < x1) issue_plane(i + 4);  // in flight during this plane's faces and update
-        const T* Pi = plane(i);
-        T* FY = FYb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFY;
-        T* FZ = FZb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFZ;
-        // GATE: a flagged face takes the characteristic-wise branch in its own lane
-        // (a dense recompute of the block's flagged faces after the pass measured
-        // slower: it adds a block-wide round and a barrier to every plane)
-        if (conv_dims > 0) {
-            if (row) xface(i, gx != 0, fxr);
-            // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
-            for (int e = rotated(tid, 7), r = 0; e < M::NFY; e += FT, r++) {
-                int fb = e / M::TZ, cz = e % M::TZ;
-                const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
-                T out[5];
-                march_face<1, CHAR, BORGES, GATE, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1,
-                                                     gy[r] != 0, out);
-#pragma unroll
-                for (int q = 0; q < 5; q++) FY[q * M::NFY + e] = out[q];
-            }
-            if (conv_dims == 3) {
-                for (int e = rotated(tid, 6), r = 0; e < M::NFZ; e += FT, r++) {
-                    int ry = e / (M::TZ + 1), fc = e % (M::TZ + 1);
-                    const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
-                    T out[5];
-                    march_face<2, CHAR, BORGES, GATE, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1,
-                                                         gz[r] != 0, out);
-#pragma unroll
-                    for (int q = 0; q < 5; q++) FZ[q * M::NFZ + e] = out[q];
-                }
-            }
-        }
-        __syncthreads();
-        if (own) {
-            const long long o = b.at(i + NG, gj + NG, gk + NG);
-            double u0[5], ui[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) {  // issued before the viscous terms hide their latency
-                u0[q] = U0[q * b.fstride + o];
-                ui[q] = Uin[q * b.fstride + o];
-            }
-            double r[5] = {0, 0, 0, 0, 0};
-            if (conv_dims > 0) {
-#pragma unroll
-                for (int q = 0; q < 5; q++) {
-                    r[q] += (double(fxr[q]) - double(fxl[q])) * c.inv_dx;
-                    r[q] += (double(FY[q * M::NFY + (ty + 1) * M::TZ + tz]) -
-                             double(FY[q * M::NFY + ty * M::TZ + tz])) * c.inv_dy;
-                    if (conv_dims == 3)
-                        r[q] += (double(FZ[q * M::NFZ + ty * (M::TZ + 1) + tz + 1]) -
-                                 double(FZ[q * M::NFZ + ty * (M::TZ + 1) + tz])) * c.inv_dz;
-                }
-            }
-            if constexpr (H > 0) {
-                T rv[5] = {0, 0, 0, 0, 0};
-                march_viscous<H, T>(plane, i, ccol, c, b.nx, b.ny, i, gj, rv);
-#pragma unroll
-                for (int q = 1; q < 5; q++) r[q] += double(rv[q]);
-            }
-            double un[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) {
-                un[q] = (u0[q] * m1) + (ui[q] * m2) + (r[q] * m3);
-                Uout[q * b.fstride + o] = un[q];
-            }
-            if constexpr (LAST) {
-                double w[5], un0[5];
-                prim_from_cons(un, c.gm1, w);
-                double d = local_dt(w, c);
-                if (d < best) best = d;
-                cons_from_prim(w, c.inv_gm1, un0);
-#pragma unroll
-                for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = un0[q];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 5; q++) fxl[q] = fxr[q];
-        if constexpr (!M::LEAN) __syncthreads();
-    }
-    if constexpr (LAST) block_min_to(best, slot_next);
-}
-
-template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool GATE>
-static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
-    using M = MarchTile<T, H>;
-    auto kern = k_stage_march<T, CHAR, BORGES, H, LAST, GATE>;
-    // the attribute is per device; setting it on every launch keeps multi-device use correct
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
-    if (e != cudaSuccess) return e;
-    dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + M::LX - 1) / M::LX);
-    kern<<<grid, FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
-                                   a.slot_next, a.clock, a.gate);
-    return cudaGetLastError();
-}
-
-template <typename T, bool CHAR, bool BORGES, bool LAST, bool GATE = false>
-static cudaError_t fused_h(const FusedArgs& a, cudaStream_t s) {
-    switch (a.visc_h) {
-        case 0: return fused_one<T, CHAR, BORGES, 0, LAST, GATE>(a, s);
-        case 1: return fused_one<T, CHAR, BORGES, 1, LAST, GATE>(a, s);
-        case 2: return fused_one<T, CHAR, BORGES, 2, LAST, GATE>(a, s);
-        default: return fused_one<T, CHAR, BORGES, 3, LAST, GATE>(a, s);
-    }
-}
-
-template <typename T>
-static cudaError_t fused_t(const FusedArgs& a, cudaStream_t s) {
-    if (a.gated) {  // learned-sensor gate: FP32 characteristic-wise form only
-        if constexpr (sizeof(T) == 8) {
-            return cudaErrorInvalidValue;
-        } else {
-            if (!a.chr) return cudaErrorInvalidValue;
-            if (a.borges)
-                return a.last ? fused_h<T, true, true, true, true>(a, s) : fused_h<T, true, true, false, true>(a, s);
-            return a.last ? fused_h<T, true, false, true, true>(a, s) : fused_h<T, true, false, false, true>(a, s);
-        }
-    }
-    if (a.chr) {
-        if (a.borges) return a.last ? fused_h<T, true, true, true>(a, s) : fused_h<T, true, true, false>(a, s);
-        return a.last ? fused_h<T, true, false, true>(a, s) : fused_h<T, true, false, false>(a, s);
-    }
-    if (a.borges) return a.last ? fused_h<T, false, true, true>(a, s) : fused_h<T, false, true, false>(a, s);
-    return a.last ? fused_h<T, false, false, true>(a, s) : fused_h<T, false, false, false>(a, s);
-}
-
 cudaError_t launch_stage_fused(const FusedArgs& a, cudaStream_t s) {
-    return a.fp32 ? fused_t<float>(a, s) : fused_t<double>(a, s);
+    return a.phys ? fused_launch<true>(a, s) : fused_launch<false>(a, s);
 }
 
 }  // namespace nsb

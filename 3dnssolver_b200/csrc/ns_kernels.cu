@@ -750,6 +750,37 @@ __global__ void __launch_bounds__(128) k_diagnostics(const double* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// state check (no reference counterpart: the reference lets NaN propagate,
+// src/time_scheme.cpp:104-117): counts the interior cells whose values are not
+// all finite or whose density or pressure is not positive.  PRIM: A is W
+// (pressure read directly), else A is U (pressure from the equation of state).
+template <bool PRIM>
+__global__ void __launch_bounds__(128) k_check_state(const double* __restrict__ A, Box b, Consts c,
+                                                     unsigned long long* __restrict__ count) {
+    const int k = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * 4 + threadIdx.y, i = blockIdx.z;
+    bool bad = false;
+    if (k < b.nz && j < b.ny) {
+        const long long o = b.at(i + NG, j + NG, k + NG);
+        double v[5];
+        bool fin = true;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            v[q] = A[q * b.fstride + o];
+            fin &= isfinite(v[q]);
+        }
+        double pr = v[1];
+        if (!PRIM) {
+            double w[5];
+            prim_from_cons(v, c.gm1, w);
+            pr = w[1];
+        }
+        bad = !fin || !(v[0] > 0.0) || !(pr > 0.0);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, bad);
+    if (threadIdx.x == 0 && m) atomicAdd(count, (unsigned long long)__popc(m));
+}
+
+// ---------------------------------------------------------------------------
 // host launchers
 
 static dim3 cell_grid(const Box& b) {  // all halo'd cells
@@ -928,6 +959,12 @@ void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_
         if (borges) { if (a.phys) xupd_h<false, true, true>(h, a, s); else xupd_h<false, true, false>(h, a, s); }
         else { if (a.phys) xupd_h<false, false, true>(h, a, s); else xupd_h<false, false, false>(h, a, s); }
     }
+}
+
+void launch_check_state(const double* A, bool prim, const Box& b, const Consts& c,
+                        unsigned long long* count, cudaStream_t s) {
+    if (prim) k_check_state<true><<<interior_grid(b), dim3(32, 4), 0, s>>>(A, b, c, count);
+    else k_check_state<false><<<interior_grid(b), dim3(32, 4), 0, s>>>(A, b, c, count);
 }
 
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s) {

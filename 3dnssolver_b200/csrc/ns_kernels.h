@@ -51,6 +51,8 @@ struct FusedArgs {
     int conv_dims;   // 0 (no convection), 2 or 3
     int visc_h;      // half width of the CD stencil, 0 without diffusion
     bool fp32, chr, borges, last;
+    bool phys;                        // physical semantics (local LF speed, textbook eigensystem,
+                                      // 3D viscous terms, multi-dimensional CFL)
     double m1, m2, mc;
     const unsigned long long* slot;   // CFL minimum of this step
     unsigned long long* slot_next;    // last stage: CFL minimum of the next step
@@ -87,6 +89,10 @@ void launch_viscous(int h, bool phys, const double* W, const Box& b, const Const
                     long long vs, cudaStream_t s);
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s);
 void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s);
+// interior cells of A (W if prim, else U) that are non-finite or have rho <= 0 or p <= 0,
+// added to *count
+void launch_check_state(const double* A, bool prim, const Box& b, const Consts& c,
+                        unsigned long long* count, cudaStream_t s);
 void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* acc, cudaStream_t s);
 
 }  // namespace nsb

@@ -336,9 +336,10 @@ __device__ __forceinline__ void face_prims(const double* __restrict__ W, const B
 }
 
 // ---------------------------------------------------------------------------
-// harvest: features + label of every face along DIR (FP64 fluxes, reference semantics)
+// harvest: features + label of every face along DIR (FP64 fluxes of the
+// context's semantics: PHYS selects the physical form's fluxes)
 
-template <int DIR, bool BORGES>
+template <int DIR, bool BORGES, bool PHYS>
 __global__ void __launch_bounds__(128) k_sensor_harvest(const double* __restrict__ W,
                                                         const double* __restrict__ U, Box b, Consts c,
                                                         FaceBox fb, long long base, double thr,
@@ -351,9 +352,9 @@ __global__ void __launch_bounds__(128) k_sensor_harvest(const double* __restrict
     long long step;
     long long o0 = face_origin<DIR>(b, aa, bb, kk, step);
     double fL[5][5], fR[5][5], wa[5], fc[5], fx[5];
-    face_stencil<DIR, true, false, double>(W, U, b, c, o0, step, fL, fR, wa);
+    face_stencil<DIR, true, PHYS, double>(W, U, b, c, o0, step, fL, fR, wa);
     face_comp<double, BORGES>(fL, fR, fc);
-    face_char<DIR, false, double, BORGES>(fL, fR, wa, c.gamma, c.inv_gm1, fx);
+    face_char<DIR, PHYS, double, BORGES>(fL, fR, wa, c.gamma, c.inv_gm1, fx);
     double dn = 0, nn = 0;
 #pragma unroll
     for (int q = 0; q < 5; q++) {
@@ -598,7 +599,7 @@ __global__ void __launch_bounds__(128) k_mlp_predict(const float* __restrict__ f
 // characteristic-wise recomputed on the flagged faces of the block (compacted
 // into a shared-memory list so the recompute runs without divergence).
 
-template <int DIR, bool BORGES>
+template <int DIR, bool BORGES, bool PHYS>
 __global__ void __launch_bounds__(128) k_face_gated(const double* __restrict__ W,
                                                     const double* __restrict__ U, Box b, Consts c,
                                                     float* __restrict__ F, FaceBox fb,
@@ -621,7 +622,7 @@ __global__ void __launch_bounds__(128) k_face_gated(const double* __restrict__ W
     if (live) {
         o0 = face_origin<DIR>(b, aa, bb, kk, step);
         float fL[5][5], fR[5][5], wa[5], out[5];
-        face_stencil<DIR, false, false, float>(W, U, b, c, o0, step, fL, fR, wa);
+        face_stencil<DIR, false, PHYS, float>(W, U, b, c, o0, step, fL, fR, wa);
         face_comp<float, BORGES>(fL, fR, out);
         long long fo = fb.at(aa, bb, kk);
 #pragma unroll
@@ -665,8 +666,8 @@ __global__ void __launch_bounds__(128) k_face_gated(const double* __restrict__ W
         long long st2;
         long long p0 = face_origin<DIR>(b, aa, b2, k2, st2);
         float fL[5][5], fR[5][5], wa[5], out[5];
-        face_stencil<DIR, true, false, float>(W, U, b, c, p0, st2, fL, fR, wa);
-        face_char<DIR, false, float, BORGES>(fL, fR, wa, float(c.gamma), float(c.inv_gm1), out);
+        face_stencil<DIR, true, PHYS, float>(W, U, b, c, p0, st2, fL, fR, wa);
+        face_char<DIR, PHYS, float, BORGES>(fL, fR, wa, float(c.gamma), float(c.inv_gm1), out);
         long long fo = fb.at(aa, b2, k2);
 #pragma unroll
         for (int qq = 0; qq < 5; qq++) F[qq * fb.fstride + fo] = out[qq];
@@ -829,21 +830,27 @@ ns_status sensor_set_weights(SensorState* st, const float* w, cudaStream_t s) {
 }
 
 ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const double* U, const Box& b,
-                           const Consts& c, double threshold, bool borges, void* F,
+                           const Consts& c, double threshold, bool borges, bool phys, void* F,
                            const FaceBox& fb, cudaStream_t s, long long* launches) {
     const float thr = (float)std::log(threshold / (1.0 - threshold));
     dim3 grid((fb.n2 + 31) / 32, (fb.n1 + 3) / 4, fb.n0), blk(32, 4);
-#define NS_GATED(D)                                                                                 \
-    do {                                                                                            \
-        if (borges)                                                                                 \
-            k_face_gated<D, true><<<grid, blk, 0, s>>>(W, U, b, c, (float*)F, fb, st->w, thr, st->flagged); \
-        else                                                                                        \
-            k_face_gated<D, false><<<grid, blk, 0, s>>>(W, U, b, c, (float*)F, fb, st->w, thr, st->flagged); \
+#define NS_GATED1(D, B, PH) \
+    k_face_gated<D, B, PH><<<grid, blk, 0, s>>>(W, U, b, c, (float*)F, fb, st->w, thr, st->flagged)
+#define NS_GATED(D)                                               \
+    do {                                                          \
+        if (phys) {                                               \
+            if (borges) NS_GATED1(D, true, true);                 \
+            else NS_GATED1(D, false, true);                       \
+        } else {                                                  \
+            if (borges) NS_GATED1(D, true, false);                \
+            else NS_GATED1(D, false, false);                      \
+        }                                                         \
     } while (0)
     if (dir == 0) NS_GATED(0);
     else if (dir == 1) NS_GATED(1);
     else NS_GATED(2);
 #undef NS_GATED
+#undef NS_GATED1
     st->faces += (unsigned long long)fb.n0 * fb.n1 * fb.n2;
     if (launches) (*launches)++;
     return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;
@@ -877,14 +884,19 @@ double sensor_last_fraction(SensorState* st) {
     return (double)n / (double)st->faces;
 }
 
-ns_status sensor_harvest(int dir, bool borges, const double* W, const double* U, const Box& b,
+ns_status sensor_harvest(int dir, bool borges, bool phys, const double* W, const double* U, const Box& b,
                          const Consts& c, const FaceBox& fb, long long base, double thr, float* feat,
                          float* label, cudaStream_t s) {
     dim3 grid((fb.n2 + 31) / 32, (fb.n1 + 3) / 4, fb.n0), blk(32, 4);
-#define NS_HARV(D)                                                                                   \
-    do {                                                                                             \
-        if (borges) k_sensor_harvest<D, true><<<grid, blk, 0, s>>>(W, U, b, c, fb, base, thr, feat, label); \
-        else k_sensor_harvest<D, false><<<grid, blk, 0, s>>>(W, U, b, c, fb, base, thr, feat, label);      \
+#define NS_HARV(D)                                                                                          \
+    do {                                                                                                    \
+        if (phys) {                                                                                         \
+            if (borges) k_sensor_harvest<D, true, true><<<grid, blk, 0, s>>>(W, U, b, c, fb, base, thr, feat, label); \
+            else k_sensor_harvest<D, false, true><<<grid, blk, 0, s>>>(W, U, b, c, fb, base, thr, feat, label);      \
+        } else {                                                                                            \
+            if (borges) k_sensor_harvest<D, true, false><<<grid, blk, 0, s>>>(W, U, b, c, fb, base, thr, feat, label); \
+            else k_sensor_harvest<D, false, false><<<grid, blk, 0, s>>>(W, U, b, c, fb, base, thr, feat, label);      \
+        }                                                                                                   \
     } while (0)
     if (dir == 0) NS_HARV(0);
     else if (dir == 1) NS_HARV(1);

@@ -15,7 +15,7 @@ void sensor_destroy(SensorState* st);
 // Gated face fluxes along axis dir: component-wise FP32 WENO on every face, the
 // characteristic-wise flux recomputed on the faces the sensor flags.
 ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const double* U, const Box& b,
-                           const Consts& c, double threshold, bool borges, void* F,
+                           const Consts& c, double threshold, bool borges, bool phys, void* F,
                            const FaceBox& fb, cudaStream_t s, long long* launches);
 // Per-step flags along axis dir for the fused stage kernel: the network on every
 // face of the step's start state U0, one byte per face (FaceBox order).  The
@@ -28,7 +28,8 @@ const unsigned char* sensor_mask(const SensorState* st, int dir);
 double sensor_last_fraction(SensorState* st);
 ns_status sensor_set_weights(SensorState* st, const float* w, cudaStream_t s);
 // features + labels of the faces along dir into feat/label starting at row base
-ns_status sensor_harvest(int dir, bool borges, const double* W, const double* U, const Box& b,
+// (labels from the FP64 fluxes of the given semantics)
+ns_status sensor_harvest(int dir, bool borges, bool phys, const double* W, const double* U, const Box& b,
                          const Consts& c, const FaceBox& fb, long long base, double thr, float* feat,
                          float* label, cudaStream_t s);
 

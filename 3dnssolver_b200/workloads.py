@@ -28,6 +28,16 @@ def splitmix64_uniform(seed, n, start=0):
     return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
+def _noise_slabs(seed, nx, ny, nz, ncomp, slab=16):
+    """Uniform [-1,1) draws, ncomp per cell in i-j-k order, one i-slab at a time
+    (the same stream as splitmix64_uniform(seed, nx*ny*nz*ncomp), bounded memory)."""
+    per = ny * nz * ncomp
+    for i0 in range(0, nx, slab):
+        i1 = min(nx, i0 + slab)
+        r = splitmix64_uniform(seed, (i1 - i0) * per, start=i0 * per)
+        yield i0, i1, r.reshape(i1 - i0, ny, nz, ncomp) * 2.0 - 1.0
+
+
 def cell_centres(n, L):
     """Cell-centred coordinates x = dx/2 + i dx (src/grid.cpp:48)."""
     d = L / n
@@ -108,17 +118,27 @@ def sod(p, seed=3, amp=0.01):
 
 
 def taylor_green(p, seed=5, mach=0.1, noise=1e-4):
-    """Compressible Taylor-Green vortex on [0,2pi]^3 with seeded velocity noise."""
+    """Compressible Taylor-Green vortex on [0,2pi]^3 with seeded velocity noise.
+
+    rho = 1, p = 1/(gamma M^2) + (cos 2x + cos 2y)(cos 2z + 2)/16,
+    u = sin x cos y cos z, v = -cos x sin y cos z, w = 0, plus uniform noise of
+    amplitude `noise` on u, v, w (three draws per cell in i-j-k order).
+    Generated one i-slab at a time, so 512^3 needs little more than the array."""
     W = _empty(p)
     nx, ny, nz = p.nx, p.ny, p.nz
-    x = cell_centres(nx, p.Lx)[:, None, None]
+    x = cell_centres(nx, p.Lx)
     y = cell_centres(ny, p.Ly)[None, :, None]
     z = cell_centres(nz, p.Lz)[None, None, :]
-    r = splitmix64_uniform(seed, nx * ny * nz * 3).reshape(nx, ny, nz, 3) * 2.0 - 1.0
     I = _interior(W)
-    I[..., 0] = 1.0
-    I[..., 1] = 1.0 / (p.gamma * mach * mach) + (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0) / 16.0
-    I[..., 2] = np.sin(x) * np.cos(y) * np.cos(z) + noise * r[..., 0]
-    I[..., 3] = -np.cos(x) * np.sin(y) * np.cos(z) + noise * r[..., 1]
-    I[..., 4] = noise * r[..., 2]
+    p0 = 1.0 / (p.gamma * mach * mach)
+    cy, sy, c2y = np.cos(y), np.sin(y), np.cos(2 * y)
+    cz, c2z = np.cos(z), np.cos(2 * z)
+    for i0, i1, r in _noise_slabs(seed, nx, ny, nz, 3):
+        xs = x[i0:i1, None, None]
+        S = I[i0:i1]
+        S[..., 0] = 1.0
+        S[..., 1] = p0 + (np.cos(2 * xs) + c2y) * (c2z + 2.0) / 16.0
+        S[..., 2] = np.sin(xs) * cy * cz + noise * r[..., 0]
+        S[..., 3] = -np.cos(xs) * sy * cz + noise * r[..., 1]
+        S[..., 4] = noise * r[..., 2]
     return W

@@ -2,21 +2,31 @@
 """Benchmark of the explicit RHS + SSP-RK3 time step on B200.
 
 Metric: cell-updates/s per RK3 stage = nx*ny*nz*3*steps / seconds.
-Workload (one "step" = one TimeScheme::step, i.e. three RK stages):
-  temporal double shear layer, 256^3 periodic cells on [0,2pi]^3, rho=1,
-  p=1/(gamma M^2) with M=0.5, seeded SplitMix64 noise 1e-3 on v and w,
-  FP64 characteristic-wise WENO-5 (Shu weights, Lax-Friedrichs splitting) +
-  second-order centered viscous terms (mu = 6.283e-4, Pr = 0.72), CFL 0.5,
-  reference semantics.  Synthetic input; the device state (2.9 GB) is larger
-  than L2, so no flush is needed between timed steps.
+Headline workload (one "step" = one TimeScheme::step, i.e. three RK stages):
+  compressible Taylor-Green vortex, 512^3 periodic cells on [0,2pi]^3, rho = 1,
+  M = 0.1, Re = 1600 (mu = 1/1600), Pr = 0.72, seeded SplitMix64 velocity
+  noise 1e-4, WENO-5 + second-order centered viscous terms, SSP-RK3 at CFL 0.5,
+  physical semantics (the reference's own semantics go non-finite on this case:
+  its Lax-Friedrichs speed is the constant 3 while c = 10).  `value` is the
+  plain FP64 characteristic-wise form; the FP32 forms and the FP32 + learned
+  sensor form are timed beside it and compared with it field by field.
+  Synthetic input: no dataset is involved.  The device state (22 GB at 512^3)
+  is larger than L2, so no flush is needed between timed steps.
+Also in the line: the Sod shock tube 512x128x128 run to t = 0.2 by every form
+(per-field L2/Linf against FP64 characteristic-wise), the sensor's training
+recipe with held-out precision/recall, the HBM roofline in algorithmic bytes
+(120 B per cell-stage: read U_stage and U0, write U_next), the compute
+roofline, the end-to-end rate through ns_time_step with host buffers, and the
+reference's own CPU TimeScheme::step timed on the host cores.
 
 Arms:
   default            our CUDA path (libns_b200.so through its C ABI)
   --impl reference   the reference's own CPU TimeScheme::step (compiled from its
-                     sources into oracle/_ref, OpenMP on all host cores)
-Multi-GPU (torchrun): every rank advances an independent replica (the path is
-single-GPU by design: no collective on the data path); value sums the ranks,
-time is the max over ranks.
+                     sources into oracle/_ref, OpenMP on all host cores), on the
+                     same workload's initial condition at 256^3 (a bounded sample)
+Multi-GPU (torchrun): every rank advances an independent replica (no
+collective on the data path of this line); value sums the ranks, time is the
+max over ranks.
 """
 import argparse
 import csv
@@ -36,15 +46,32 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s per RK3 stage on 1 B200 (FP32+learned vs plain FP64) at stated L2 err"
 UNIT = "cell-updates/s"
+BYTES_PER_CELL_STAGE = 120  # read U_stage and U0, write U_next: 3 x 5 doubles
 
-FORMS = {
-    # name: (convection, precision, sensor, dtype label)
-    "fp64_char": (2, 0, 0, "f64"),
-    "fp64_comp": (1, 0, 0, "f64"),
-    "fp32_char": (2, 1, 0, "f32 (f64 RK3 accumulation and reductions)"),
-    "fp32_comp": (1, 1, 0, "f32 (f64 RK3 accumulation and reductions)"),
-    "fp32_sensor": (2, 1, 1, "f32 + bf16 sensor (f64 RK3 accumulation and reductions)"),
+# workloads: initial condition, grid, semantics and physical parameters
+WORKLOADS = {
+    "tgv": dict(ic="taylor_green", n=512, semantics=1, mu=1.0 / 1600.0, Pr=0.72, cfl=0.5,
+                label="taylor_green {n}^3 periodic [0,2pi]^3 M=0.1 Re=1600, {form} WENO-5 + CD-{order} "
+                      "viscous, SSP-RK3 CFL 0.5, physical semantics"),
+    "shear": dict(ic="shear_layer", n=256, semantics=0, mu=2.0 * 0.05 * 2 * math.pi / 1000.0, Pr=0.72,
+                  cfl=0.5, label="shear_layer {n}^3 periodic [0,2pi]^3 M=0.5 Re=1000, {form} WENO-5 (LF alpha=3) "
+                                 "+ CD-{order} viscous, SSP-RK3 CFL 0.5, reference semantics"),
 }
+
+# forms: scheme, precision, sensor; `ref` is the form its state is compared with
+FORMS = {
+    "fp64_char": dict(conv=2, prec=0, dtype="f64"),
+    "fp64_comp": dict(conv=1, prec=0, dtype="f64"),
+    "fp32_char": dict(conv=2, prec=1, dtype="f32 (f64 RK3 accumulation and reductions)"),
+    "fp32_comp": dict(conv=1, prec=1, dtype="f32 (f64 RK3 accumulation and reductions)"),
+    "fp32_sensor": dict(conv=2, prec=1, sensor=1,
+                        dtype="f32 + bf16 sensor (f64 RK3 accumulation and reductions)"),
+    # the rest of the operator surface at full size: CD-6 viscous terms and Borges weights
+    "fp64_char_cd6_borges": dict(conv=2, prec=0, order=6, weights=1, ref=None, dtype="f64"),
+    "fp32_char_cd6_borges": dict(conv=2, prec=1, order=6, weights=1, ref="fp64_char_cd6_borges",
+                                 dtype="f32 (f64 RK3 accumulation and reductions)"),
+}
+FIELDS = ["rho", "rhoE", "rhou", "rhov", "rhow"]
 
 
 def parse():
@@ -53,27 +80,37 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="cells per axis of the shear-layer box")
+    ap.add_argument("--workload", default="tgv", choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=0, help="cells per axis (0: the workload's own)")
     ap.add_argument("--form", default="fp64_char", choices=sorted(FORMS))
-    ap.add_argument("--also", default="fp64_comp,fp32_char,fp32_comp,fp32_sensor",
+    ap.add_argument("--also", default="fp64_comp,fp32_char,fp32_comp,fp32_sensor,fp64_char_cd6_borges,"
+                                      "fp32_char_cd6_borges",
                     help="extra forms timed after the headline (comma list, '' for none)")
+    ap.add_argument("--accuracy-steps", type=int, default=0,
+                    help="steps of the per-form accuracy runs (0: warmup + steps)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sod", action="store_true", help="skip the 512x128x128 Sod comparison")
+    ap.add_argument("--cpu-sample-n", type=int, default=256,
+                    help="grid of the reference CPU sample (the same workload's IC)")
     return ap.parse_args()
 
 
-def workload_params(pkg, n, form):
-    conv, prec, sensor, _ = FORMS[form]
+def workload_params(pkg, wk, n, form):
+    W, F = WORKLOADS[wk], FORMS[form]
     L = 2 * math.pi
-    # mu = rho0 * dU * delta / Re with dU = 2, delta = 0.05*2pi, Re = 1000
-    return pkg.make_params(n, n, n, L=(L, L, L), mu=2.0 * 0.05 * 2 * math.pi / 1000.0, Pr=0.72,
-                           gamma=1.4, cfl=0.5, convection=conv, diffusion_order=2, precision=prec,
-                           sensor=sensor)
+    return pkg.make_params(n, n, n, L=(L, L, L), mu=W["mu"], Pr=W["Pr"], gamma=1.4, cfl=W["cfl"],
+                           convection=F["conv"], weights=F.get("weights", 0),
+                           diffusion_order=F.get("order", 2), precision=F["prec"],
+                           semantics=W["semantics"], sensor=F.get("sensor", 0))
 
 
-def workload_name(n, form):
-    return (f"shear_layer {n}^3 periodic [0,2pi]^3 M=0.5 Re=1000, {form} WENO-5 (Shu, LF alpha=3) "
-            f"+ CD-2 viscous, SSP-RK3 CFL 0.5, reference semantics")
+def workload_name(wk, n, form):
+    return WORKLOADS[wk]["label"].format(n=n, form=form, order=FORMS[form].get("order", 2))
+
+
+def initial_state(wl, wk, p, seed):
+    return getattr(wl, WORKLOADS[wk]["ic"])(p, seed=seed)
 
 
 # ---------------------------------------------------------------------------
@@ -130,38 +167,46 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's own TimeScheme::step (oracle/_ref) on host cores
+# the reference's own TimeScheme::step (oracle/_ref) on host cores
 
-def cpu_baseline(steps=2, warmup=1, n=256):
+def _ref_cpu_params(pkg, wk, n):
+    # the reference has one semantics; the same initial condition and schemes otherwise
+    p = workload_params(pkg, wk, n, "fp64_char")
+    p.semantics = 0
+    return p
+
+
+def _ref_sample_text(wk, n, n_full, threads, steps):
+    extra = ""
+    if WORKLOADS[wk]["semantics"] == 1:
+        extra = (" with the reference's own semantics (it has no physical form; its characteristic-wise "
+                 "Taylor-Green run turns non-finite after a few tens of steps, which does not change the "
+                 "work or the time of a step)")
+    return (f"{steps} timed TimeScheme::step calls on the {WORKLOADS[wk]['ic']} initial condition at {n}^3 "
+            f"({(n / n_full) ** 3:.3g} of the workload's {n_full}^3 cells){extra}; "
+            f"reference sources built with -O3 -ffast-math -march=x86-64-v3 (its CMake uses -march=native; "
+            f"x86-64-v3 so that the binary built here runs on the GPU host), OpenMP {threads} threads, 1 rank")
+
+
+def cpu_baseline(pkg, wk, n, n_full, steps=2, warmup=1):
     from oracle import oracle as O
-    pkg = importlib.import_module("3dnssolver_b200")
     threads = os.cpu_count() or 1
-    p = workload_params(pkg, n, "fp64_char")
-    if O.ref_available(strict=False):
-        r = O.ref_bench(p, steps=steps, warmup=warmup, threads=threads, timed=True)
-        return {"value": r["cell_updates_per_s"], "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"{steps} timed TimeScheme::step calls (after {warmup} warm-up) of the "
-                          f"same workload at {n}^3, reference sources built with -O3 -ffast-math, "
-                          f"OpenMP {threads} threads, 1 rank", "seconds": r["seconds"]}
-    # the oracle port (strict IEEE C restatement) when the reference build is absent
-    wl = importlib.import_module("3dnssolver_b200.workloads")
-    n = 64
-    p = workload_params(pkg, n, "fp64_char")
-    W = wl.shear_layer(p, seed=1)
-    O.run(p, W, 1)
-    t0 = time.perf_counter()
-    O.run(p, W, steps)
-    sec = time.perf_counter() - t0
-    return {"value": n ** 3 * 3 * steps / sec, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{steps} steps at {n}^3 of the oracle port", "seconds": sec}
+    if not O.ref_available(strict=False):
+        return {"error": "oracle/_ref/ref_harness_timed is not built (needs the reference tree)"}
+    p = _ref_cpu_params(pkg, wk, n)
+    r = O.ref_bench(p, steps=steps, warmup=warmup, threads=threads, timed=True,
+                    ic="tgv" if WORKLOADS[wk]["ic"] == "taylor_green" else "shear")
+    return {"value": r["cell_updates_per_s"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": _ref_sample_text(wk, n, n_full, threads, steps), "seconds": r["seconds"]}
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    # sample grid: keep the whole --warmup/--steps run within a few minutes
-    n = 256 if args.warmup + args.steps <= 16 else 128
+    wk = args.workload
+    n_full = args.n or WORKLOADS[wk]["n"]
+    n = min(args.cpu_sample_n, n_full)
     try:
         from oracle import oracle as O
         if not O.ref_available(strict=False):
@@ -169,23 +214,23 @@ def reference_arm(args):
                               "oracle/_ref/ref_harness_timed not built (needs the reference tree)"}))
             return 0
         pkg = importlib.import_module("3dnssolver_b200")
-        p = workload_params(pkg, n, "fp64_char")
         threads = os.cpu_count() or 1
-        r = O.ref_bench(p, steps=args.steps, warmup=args.warmup, threads=threads, timed=True)
+        p = _ref_cpu_params(pkg, wk, n)
+        r = O.ref_bench(p, steps=args.steps, warmup=args.warmup, threads=threads, timed=True,
+                        ic="tgv" if WORKLOADS[wk]["ic"] == "taylor_green" else "shear")
     except Exception as e:  # report, do not crash the driver
         print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {e}"}))
         return 0
     v = r["cell_updates_per_s"]
+    sample = _ref_sample_text(wk, n, n_full, threads, args.steps)
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * r["seconds"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.n, "fp64_char"), "sample_grid": [n, n, n],
-                   "parallelism": "1 rank, OpenMP"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"each step one TimeScheme::step at {n}^3 (reference sources, "
-                                   f"-O3 -ffast-math, OpenMP {threads} threads)"},
+        "config": {"workload": workload_name(wk, n_full, "fp64_char"), "grid": [n_full] * 3,
+                   "sample_grid": [n, n, n], "sample": sample, "parallelism": "1 rank, OpenMP"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -211,14 +256,13 @@ def job_rate(world, cells, steps, ms_max):
 
 
 # ---------------------------------------------------------------------------
-# rooflines of the dominant kernel
+# rooflines
 
 # Floating-point work per unit of each kernel class, counted by ncu on the 128^3
-# shear layer (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}[2]_pred_on.sum
+# shear layer, reference semantics (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}[2]_pred_on.sum
 # divided by the faces or cells of the launch; the counts do not depend on the data):
 # (flop per unit with an FMA as 2, FP lane operations per unit with a packed f32x2
-# operation as 2, pipe, unit).  The fused stage rows are the first two stages; the
-# third adds the next step's start (about 70 FP64 instructions per cell).
+# operation as 2, pipe, unit).  The fused stage rows are the first two stages.
 COMPUTE_PER_UNIT = {
     ("fp64_char", "face_x"): (1325, 953, "fp64", "face"),
     ("fp64_char", "face_y"): (1325, 953, "fp64", "face"),
@@ -228,17 +272,15 @@ COMPUTE_PER_UNIT = {
     ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
     ("fp64_char", "update"): (316, 205, "fp64", "cell"),
     ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
-    # x-faces marched with the update (second stage; measured per cell)
     ("fp64_char", "xface_update"): (1505, 1083, "fp64", "cell"),
     ("fp64_comp", "xface_update"): (1155, 856, "fp64", "cell"),
-    # viscous terms, CD-2 reference semantics (measured per cell)
     ("fp64_char", "viscous"): (222, 135, "fp64", "cell"),
     ("fp64_comp", "viscous"): (222, 135, "fp64", "cell"),
     ("fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
     ("fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
 }
-# DRAM bytes (read + write) per unit from the same capture; these kernels stream
-# their inputs once at 128^3 and above, so the traffic scales with the units.
+# DRAM bytes (read + write) per unit from one ncu capture at 128^3 (the kernels
+# stream their inputs once at 128^3 and above, so traffic scales with the units).
 TRAFFIC_PER_UNIT = {
     ("fp64_char", "face_x"): 120.4, ("fp64_char", "face_y"): 118.6, ("fp64_char", "face_z"): 113.6,
     ("fp64_comp", "face_x"): 119.7, ("fp64_comp", "face_y"): 118.7, ("fp64_comp", "face_z"): 113.3,
@@ -246,6 +288,10 @@ TRAFFIC_PER_UNIT = {
     ("fp64_char", "xface_update"): 332.7, ("fp64_comp", "xface_update"): 330.3,
     ("fp64_char", "viscous"): 51.2, ("fp64_comp", "viscous"): 51.2,
 }
+KERNEL_NAMES = {"stage_fused": "k_stage_march", "update": "k_update", "sensor": "k_sensor_mask",
+                "xface_update": "k_xface_update", "viscous": "k_viscous", "fill_prim": "k_fill_prim/k_fill_halo",
+                "step_begin": "k_step_begin", "face_x": "k_face_flux<x>", "face_y": "k_face_flux<y>",
+                "face_z": "k_face_flux<z>"}
 
 
 def profile(s, reps=3):
@@ -254,61 +300,164 @@ def profile(s, reps=3):
     return {k: statistics.mean(pr[k] for pr in profs) for k in profs[0]}
 
 
-def rooflines(form, prof, n, peaks, fma):
-    """HBM and compute rooflines of the form's dominant kernel class."""
+def rooflines(form, prof, n, ms_per_step, peaks, fma):
+    """HBM roofline (algorithmic bytes: 120 B per cell-stage) of the form's dominant
+    kernel class and of the whole step, and the compute roofline of that kernel."""
     cells = n ** 3
+    faces = (n + 1) * n * n
     dom = max(prof, key=prof.get)
     launches = 1 if dom == "step_begin" else 3
     per_launch_ms = prof[dom] / launches
-    # algorithmic bytes: a face-flux launch reads W and U (2 x 5 doubles per cell) and
-    # writes 5 values per face; an update launch reads U, U0 and 3 face arrays and
-    # writes U; a fused stage reads U_in and U0 and writes U_out: 120 B per cell (the
-    # third stage also writes the next step's U0; the common 120 B/cell-stage unit is kept)
-    elem = 4 if FORMS[form][1] == 1 else 8
-    faces = (n + 1) * n * n
-    face_bytes = cells * 80 + faces * 5 * elem
-    alg = {"face_x": face_bytes, "face_y": face_bytes, "face_z": face_bytes,
-           "update": cells * (3 * 40) + 3 * faces * 5 * elem + cells * 40,
-           "fill_prim": (n + 6) ** 3 * 80, "step_begin": (n + 6) ** 3 * 120,
-           "stage_fused": cells * 120,
-           # per-step sensor flags: U0 read once per axis, one byte per face written
-           "sensor": 3 * (cells * 40 + faces),
-           # x-faces + update: W and U (x stencils), the y- and z-face fluxes and U0
-           # read, U_out and the next stage's W written (+ the 4 viscous terms read)
-           "xface_update": cells * 312,
-           # viscous terms: W (rho, p, u, v) read, 4 doubles written per cell
-           "viscous": cells * 64}
-    kname = {"stage_fused": f"k_stage_march ({form})", "update": f"k_update ({form})",
-             "sensor": f"k_sensor_mask ({form})", "xface_update": f"k_xface_update ({form})",
-             "viscous": f"k_viscous ({form})"}.get(
-        dom, f"k_face_flux ({dom}, {form})" if dom.startswith("face") else dom)
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = alg[dom] / (per_launch_ms / 1000.0) / 1e9
+    alg = BYTES_PER_CELL_STAGE * cells  # one stage of every cell per launch
+    achieved = alg / (per_launch_ms / 1e3) / 1e9
     units = faces if dom.startswith("face") else cells
-    tpu = TRAFFIC_PER_UNIT.get((form, dom))
+    key = ("fp64_char" if form.startswith("fp64_char") else form.split("_cd6")[0], dom)
+    tpu = TRAFFIC_PER_UNIT.get(key)
+    traffic = round(tpu * units) if tpu else None
+    step_alg = 3 * alg
+    step_achieved = step_alg / (ms_per_step / 1e3) / 1e9
+    # measured traffic of all kernel classes of one step where the capture has them
+    step_traffic = 0.0
+    covered = True
+    for cls, ms in prof.items():
+        if ms <= 0:
+            continue
+        t = TRAFFIC_PER_UNIT.get((key[0], cls))
+        if t is None:
+            covered = False
+            continue
+        step_traffic += t * (faces if cls.startswith("face") else cells) * (1 if cls == "step_begin" else 3)
+    kname = KERNEL_NAMES.get(dom, dom) + f" ({form})"
     hbm = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-           "frac": round(achieved / hbm_peak, 4),
-           "traffic": round(tpu * units) if tpu else None,
-           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit at 128^3, "
-                             "scaled by the units of this launch" if tpu else None,
+           "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
+           "traffic_over_algorithmic": round(traffic / alg, 3) if traffic else None,
+           "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum per unit at 128^3, "
+                              "scaled by the units of this launch") if tpu else None,
            "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s",
-           "algorithmic_bytes_per_launch": alg[dom], "launch_ms": round(per_launch_ms, 4)}
+           "algorithmic_bytes_per_launch": alg,
+           "algorithmic_unit": "120 B per cell-stage (U_stage and U0 read, U_next written) x cells",
+           "launch_ms": round(per_launch_ms, 4),
+           "step": {"achieved": round(step_achieved, 1), "frac": round(step_achieved / hbm_peak, 4),
+                    "algorithmic_bytes": step_alg,
+                    "measured_traffic": round(step_traffic) if covered and step_traffic else None,
+                    "traffic_over_algorithmic": round(step_traffic / step_alg, 3)
+                    if covered and step_traffic else None}}
     comp = None
-    row = COMPUTE_PER_UNIT.get((form, dom))
+    row = COMPUTE_PER_UNIT.get(key)
     if row:
         flop_u, inst_u, pipe, unit = row
         peak = fma[pipe]
-        tflops = flop_u * units / (per_launch_ms / 1000.0) / 1e12
+        tflops = flop_u * units / (per_launch_ms / 1e3) / 1e12
         # FP lane operations against the FMA rate (peak / 2 flops): a multiply or add
         # takes the same pipe slot as an FMA, so this is the pipe's busy fraction
-        ops_rate = inst_u * units / (per_launch_ms / 1000.0) / 1e12
+        ops_rate = inst_u * units / (per_launch_ms / 1e3) / 1e12
         comp = {"bound": pipe, "kernel": kname, "achieved": round(tflops, 2), "peak": round(peak, 2),
                 "unit": "TFLOP/s", "frac": round(tflops / peak, 4),
                 "pipe_frac": round(ops_rate / (peak / 2.0), 4),
                 "peak_source": f"measured now: ns_fma_peak ({pipe} FMA chains on every SM)",
+                "counts_source": "ncu per-opcode counts of the reference-semantics kernel at 128^3",
                 "flop_per_" + unit: flop_u, "fp_ops_per_" + unit: inst_u}
         hbm["note"] = f"{pipe}-pipe bound: see compute_roofline"
     return hbm, comp
+
+
+# ---------------------------------------------------------------------------
+# accuracy: per-field errors against the comparison form, on the GPU
+
+def interior_tensor(U):
+    import torch
+    return torch.from_numpy(U[3:-3, 3:-3, 3:-3]).cuda()
+
+
+def field_errors(U, R):
+    """Relative L2 and Linf of U against R per conserved field; the momentum
+    components also against the momentum magnitude (a field like rhow can be
+    noise-amplitude, where its own norm is no scale)."""
+    import torch
+    out = {"rel_l2": {}, "rel_linf": {}, "mom_l2": {}, "mom_linf": {}}
+    mom_l2 = math.sqrt(float((R[..., 2:5] ** 2).sum().item()))
+    mom_inf = float(torch.sqrt((R[..., 2:5] ** 2).sum(-1)).max().item())
+    for q, f in enumerate(FIELDS):
+        d = U[..., q] - R[..., q]
+        l2 = math.sqrt(float((d * d).sum().item()))
+        li = float(d.abs().max().item())
+        out["rel_l2"][f] = l2 / max(math.sqrt(float((R[..., q] ** 2).sum().item())), 1e-300)
+        out["rel_linf"][f] = li / max(float(R[..., q].abs().max().item()), 1e-300)
+        if q >= 2:
+            out["mom_l2"][f] = l2 / max(mom_l2, 1e-300)
+            out["mom_linf"][f] = li / max(mom_inf, 1e-300)
+    return out
+
+
+def accuracy_run(pkg, params, W0, steps, sensor_w=None, every=1):
+    """Advances a fresh context `steps` steps from W0, recording time, kinetic energy and
+    enstrophy every `every` steps; returns (interior U on the GPU, history)."""
+    hist = {"step": [], "time": [], "kinetic": [], "enstrophy": []}
+    with pkg.Solver(params) as s:
+        if sensor_w is not None:
+            s.set_sensor_weights(sensor_w)
+        s.upload_primitive(W0)
+        d = s.diagnostics()
+        for k in range(steps + 1):
+            if k % every == 0 or k == steps:
+                d = s.diagnostics()
+                hist["step"].append(k)
+                hist["time"].append(d["time"])
+                hist["kinetic"].append(d["kinetic"])
+                hist["enstrophy"].append(d["enstrophy"])
+            if k < steps:
+                s.advance(1)
+        frac = d["sensor_fraction"]
+        U = interior_tensor(s.download_conservative())
+    return U, hist, frac
+
+
+def sod_comparison(pkg, wl, sensor_w_ref, t_end=0.2):
+    """The 512x128x128 Sod shock tube (Ly = Lz = 1, characteristic-wise, CFL 0.4,
+    reference semantics) to t = 0.2 in every form; errors against FP64 characteristic-wise."""
+    import torch
+    sensor_mod = importlib.import_module("3dnssolver_b200.sensor")
+    base = sensor_mod.sod_params(512, 128, 128)
+    W0 = wl.sod(base, seed=3)
+    out = {"workload": "sod 512x128x128, x in [0,1] (Neumann), y,z in [0,1] periodic (dy = dz = 4 dx), "
+                       "interface x = 0.5 + 0.01 sin(2 pi y) sin(2 pi z), mu = 1e-4, CD-2, CFL 0.4, "
+                       "reference semantics (Ly = Lz = 1: stable at CFL 0.4 under its min-over-axes dt)",
+           "t_end": t_end, "forms": {}}
+    # the FP64 characteristic-wise run sets the step count that reaches t_end
+    with pkg.Solver(base) as s:
+        s.upload_primitive(W0)
+        steps, t = 0, 0.0
+        while t < t_end and steps < 5000:
+            s.advance(1)
+            steps += 1
+            t = s.get_dt()[1]
+        Uref = interior_tensor(s.download_conservative())
+    out["steps"], out["t_fp64_char"] = steps, t
+    for form, kw in [("fp64_comp", dict(convection=1)), ("fp32_char", dict(precision=1)),
+                     ("fp32_comp", dict(precision=1, convection=1)),
+                     ("fp32_sensor", dict(precision=1, sensor=1))]:
+        p = sensor_mod.sod_params(512, 128, 128, **kw)
+        with pkg.Solver(p) as s:
+            if kw.get("sensor"):
+                s.set_sensor_weights(sensor_w_ref)
+            s.upload_primitive(W0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.advance(steps)
+            s.synchronize()
+            sec = time.perf_counter() - t0
+            d = s.diagnostics()
+            U = interior_tensor(s.download_conservative())
+        e = field_errors(U, Uref)
+        e["time"] = d["time"]
+        e["sensor_fraction"] = d["sensor_fraction"] if kw.get("sensor") else None
+        e["cell_updates_per_s"] = 512 * 128 * 128 * 3 * steps / sec
+        out["forms"][form] = e
+        del U
+    del Uref
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -316,7 +465,6 @@ def main():
     if args.impl == "reference":
         return reference_arm(args)
 
-    import numpy as np
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -339,28 +487,31 @@ def main():
 
     pkg = importlib.import_module("3dnssolver_b200")
     wl = importlib.import_module("3dnssolver_b200.workloads")
-    n = args.n
+    sensor_mod = importlib.import_module("3dnssolver_b200.sensor")
+    wk = args.workload
+    n = args.n or WORKLOADS[wk]["n"]
     cells = n ** 3
-    p = workload_params(pkg, n, args.form)
-    W0 = wl.shear_layer(p, seed=1 + rank)
+    p = workload_params(pkg, wk, n, args.form)
+    W0 = initial_state(wl, wk, p, seed=(5 if wk == "tgv" else 1) + rank)
     # a dedicated stream: the context adopts it, so CUDA events recorded on it bracket
     # exactly the library's kernels (torch's default stream is the legacy NULL stream)
     stream = torch.cuda.Stream()
+    forms_wanted = [args.form] + [f for f in args.also.split(",") if f and f != args.form]
 
-    sensor_w, sensor_info = None, None
+    # the learned sensor, trained by its recipe in the semantics of each workload that uses it
+    sensor_w, sensor_info = {}, {}
+
+    def sensor_weights(sem):
+        if sem not in sensor_w:
+            sensor_w[sem], sensor_info[sem] = sensor_mod.train_recipe(semantics=sem, seed=0)
+        return sensor_w[sem]
 
     def time_form(form, steps, warmup, sample_clocks=False):
-        nonlocal sensor_w, sensor_info
-        pf = workload_params(pkg, n, form)
-        if FORMS[form][2] and sensor_w is None:
-            sensor_mod = importlib.import_module("3dnssolver_b200.sensor")
-            X, y = sensor_mod.default_training_set()
-            sensor_w, sensor_info = sensor_mod.train(X, y, seed=0)
-            del X, y
+        pf = workload_params(pkg, wk, n, form)
         s = pkg.Solver(pf)
         s.set_stream(stream.cuda_stream)
-        if FORMS[form][2]:
-            s.set_sensor_weights(sensor_w)
+        if FORMS[form].get("sensor"):
+            s.set_sensor_weights(sensor_weights(WORKLOADS[wk]["semantics"]))
         s.upload_primitive(W0)
         s.advance(warmup)
         torch.cuda.synchronize()
@@ -371,7 +522,7 @@ def main():
             # sees the GPU under this load right up to and through the timed region
             t0 = time.time()
             while time.time() - t0 < 1.0:
-                s.advance(2)
+                s.advance(1)
                 torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
@@ -385,22 +536,23 @@ def main():
         ms = e0.elapsed_time(e1)
         launches = s.launches - l0
         clocks = clk.stop() if clk else None
-        diag = s.diagnostics()
-        return s, ms, launches, clocks, diag
+        return s, ms, launches, clocks
 
-    s, ms, launches, clocks, diag = time_form(args.form, args.steps, args.warmup, sample_clocks=True)
-    ms_max = rank_max(ms)
-    value = job_rate(world, cells, args.steps, ms_max)
-
-    # per-kernel device times of one step (events between kernels on the same stream)
-    prof = profile(s)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     fma = {"fp64": pkg.fma_peak(True), "fp32": pkg.fma_peak(False)}
-    roofline, compute_roofline = rooflines(args.form, prof, n, peaks, fma)
+
+    # ---- headline form: timed, profiled, then the end-to-end rate
+    if FORMS[args.form].get("sensor"):
+        sensor_weights(WORKLOADS[wk]["semantics"])
+    s, ms, launches, clocks = time_form(args.form, args.steps, args.warmup, sample_clocks=True)
+    ms_max = rank_max(ms)
+    value = job_rate(world, cells, args.steps, ms_max)
+    prof = profile(s)
+    roofline, compute_roofline = rooflines(args.form, prof, n, ms_max / args.steps, peaks, fma)
 
     # end to end through the C ABI with host buffers: ns_time_step uploads W from pinned
     # host memory, runs the step and downloads W every step
@@ -422,49 +574,57 @@ def main():
            "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Wh.nbytes),
            "steps": args.e2e_steps, "api": "ns_time_step (TimeScheme::step drop-in), pinned host W"}
     s.close()
+    del Wh, Wh_t
 
-    # extra forms on the same workload (same timing rules); every form advances the
-    # same initial state by warmup + steps steps, so their states compare with the
-    # headline form's: relative L2 error per conserved field against it
-    g3 = slice(3, -3)
-    forms = {args.form: {"value": value, "ms_per_step": ms_max / args.steps}}
-    if FORMS[args.form][2]:
-        forms[args.form]["sensor_fraction"] = diag["sensor_fraction"]
-        forms[args.form]["sensor_training"] = sensor_info
-    U_ref = None
-    if args.also:
-        s0 = pkg.Solver(p)
-        if FORMS[args.form][2]:
-            s0.set_sensor_weights(sensor_w)
-        s0.upload_primitive(W0)
-        s0.advance(args.warmup + args.steps)
-        U_ref = s0.download_conservative()[g3, g3, g3]
-        s0.close()
-    names = ["rho", "rhoE", "rhou", "rhov", "rhow"]
-    for f in [x for x in args.also.split(",") if x and x != args.form]:
+    forms = {args.form: {"value": value, "ms_per_step": ms_max / args.steps, "gpu_launches": launches,
+                         "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items() if v > 0}}}
+    for f in forms_wanted[1:]:
         try:
-            s2, ms2, l2, _, d2 = time_form(f, args.steps, args.warmup)
-            U2 = s2.download_conservative()[g3, g3, g3]
-            hbm2, comp2 = rooflines(f, profile(s2), n, peaks, fma)
-            s2.close()
+            s2, ms2, l2, _ = time_form(f, args.steps, args.warmup)
             ms2 = rank_max(ms2)
-            num = np.sqrt(((U2 - U_ref) ** 2).reshape(-1, 5).sum(0))
-            den = np.sqrt((U_ref ** 2).reshape(-1, 5).sum(0))
-            forms[f] = {"value": job_rate(world, cells, args.steps, ms2),
-                        "ms_per_step": ms2 / args.steps, "gpu_launches": l2,
-                        "rel_l2_vs_" + args.form: {k: float(v) for k, v in zip(names, num / den)},
+            pr2 = profile(s2)
+            hbm2, comp2 = rooflines(f, pr2, n, ms2 / args.steps, peaks, fma)
+            s2.close()
+            forms[f] = {"value": job_rate(world, cells, args.steps, ms2), "ms_per_step": ms2 / args.steps,
+                        "gpu_launches": l2, "vs_" + args.form: ms_max / ms2,
+                        "kernel_ms_per_step": {k: round(v, 4) for k, v in pr2.items() if v > 0},
                         "roofline": hbm2, "compute_roofline": comp2}
-            if FORMS[f][2]:
-                forms[f]["sensor_fraction"] = d2["sensor_fraction"]
-                forms[f]["sensor_training"] = sensor_info
         except Exception as e:
             forms[f] = {"error": str(e)}
-    del U_ref
+
+    # ---- accuracy: every form advances the same initial state; errors against its comparison form
+    acc_steps = args.accuracy_steps or (args.warmup + args.steps)
+    every = max(1, acc_steps // 50)
+    refs = {}
+    for f in forms_wanted:
+        if "error" in forms[f]:
+            continue
+        pf = workload_params(pkg, wk, n, f)
+        sw = sensor_weights(WORKLOADS[wk]["semantics"]) if FORMS[f].get("sensor") else None
+        U, hist, frac = accuracy_run(pkg, pf, W0, acc_steps, sensor_w=sw, every=every)
+        forms[f]["history"] = hist
+        if FORMS[f].get("sensor"):
+            forms[f]["sensor_fraction"] = frac
+        ref = FORMS[f].get("ref", args.form)
+        if ref is not None and ref != f and ref in refs:
+            forms[f]["errors_vs_" + ref] = dict(field_errors(U, refs[ref]), steps=acc_steps)
+        if f == args.form or any(FORMS[g].get("ref", args.form) == f for g in forms_wanted if g != f):
+            refs[f] = U  # a later form is compared with this one
+        del U
+    refs.clear()
+    torch.cuda.empty_cache()
+
+    sod = None
+    if rank == 0 and not args.no_sod:
+        try:
+            sod = sod_comparison(pkg, wl, sensor_weights(0))
+        except Exception as e:
+            sod = {"error": str(e)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_baseline(n=n)
+            cpu = cpu_baseline(pkg, wk, min(args.cpu_sample_n, n), n)
         except Exception as e:
             cpu = {"error": str(e)}
 
@@ -472,16 +632,16 @@ def main():
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": FORMS[args.form][3], "data": "synthetic",
-            "config": {"workload": workload_name(n, args.form), "grid": [n, n, n], "form": args.form,
-                       "l2": "no flush: device state 2.9 GB > 126 MB L2",
+            "scaling": "weak", "vs_baseline": None, "dtype": FORMS[args.form]["dtype"], "data": "synthetic",
+            "config": {"workload": workload_name(wk, n, args.form), "grid": [n, n, n], "form": args.form,
+                       "l2": f"no flush: device state {5 * 8 * (n + 6) ** 3 * 4 / 1e9:.1f} GB > 126 MB L2",
                        "parallelism": f"{world} independent replica(s), no data-path collective"},
             "roofline": roofline, "compute_roofline": compute_roofline,
-            "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
+            "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items() if v > 0},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "forms": forms,
-            "diagnostics": {"nonfinite": diag["nonfinite"], "dt": diag["dt"],
-                            "mass": diag["mass"], "kinetic": diag["kinetic"]},
+            "sensor_training": {("physical" if k else "reference"): v for k, v in sensor_info.items()},
+            "sod_512x128x128": sod,
         }
         print(json.dumps(out))
     if dist is not None:

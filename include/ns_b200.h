@@ -82,7 +82,11 @@ typedef struct ns_params {
     int semantics;       /* NS_SEM_* */
     int sensor;          /* 1: learned sensor gates the characteristic projection (FP32 only) */
     double sensor_threshold; /* sensor fires when sigmoid(logit) > threshold (default 0.5) */
-    int reserved[8];
+    int check_finite;    /* 1: ns_advance, ns_time_step and ns_synchronize check the state and
+                          * return NS_ERR_NONFINITE if an interior cell holds NaN/Inf or a
+                          * non-positive density or pressure (the reference lets NaN propagate
+                          * silently, src/time_scheme.cpp:104-117); 0 (default): no check */
+    int reserved[7];
 } ns_params;
 
 /* Global diagnostics of the device state (no reference counterpart: the
@@ -151,14 +155,18 @@ NS_API ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out)
 /* ---- device-resident time loop -------------------------------------------- */
 /* Runs nsteps steps of TimeScheme::step on the device-resident state (the Driver
  * loop, src/driver.cpp:43-68, without host copies).  Asynchronous on the
- * context's stream; no host synchronisation inside. */
+ * context's stream; no host synchronisation inside, unless params.check_finite
+ * is set: then the call waits for the steps and checks the state
+ * (NS_ERR_NONFINITE, see ns_synchronize). */
 NS_API ns_status ns_advance(ns_ctx* ctx, int nsteps);
 /* dt of the last step and the sum of dt over the steps taken (0 before the
  * first step): TimeScheme::get_dt (src/time_scheme.hpp:31) plus the Driver's
  * time accumulation (src/driver.cpp:54-58).  Waits for the context's stream. */
 NS_API ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time);
-/* Blocks until the context's stream is idle; NS_ERR_NONFINITE if
- * check_finite was requested and the state holds NaN/Inf. */
+/* Blocks until the context's stream is idle.  With params.check_finite set it
+ * then checks the current state: NS_ERR_NONFINITE if an interior cell holds
+ * NaN/Inf or a non-positive density or pressure (the message gives the number
+ * of such cells).  ns_time_step runs the same check after its step. */
 NS_API ns_status ns_synchronize(ns_ctx* ctx);
 NS_API ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
 /* Kernel classes timed by ns_profile_step (NS_PROF_SENSOR: the per-step
@@ -227,13 +235,17 @@ NS_API ns_status ns_set_sensor_weights(ns_ctx* ctx, const float* w);
  * box (nx+6) x (ny+6) x (nz+6) doubles with k fastest; work is queued on
  * cuda_stream (NULL: the legacy default stream) and the call returns without
  * waiting.  The face fluxes live in one array of NS_NOALLOC_SCRATCH_BYTES
- * compiled into the library, held on every GPU that loads it until the
- * process exits; grids whose face fluxes do not fit (beyond about 64^3 cells
- * in FP64) are rejected with NS_ERR_INVALID_ARG.  The first call on each
- * device looks up that array's device address; make that first call before
- * any stream capture begins.  All calls on a device share the array: calls
- * that overlap on the GPU race, so serialise them.  Nothing is allocated:
- * no cudaMalloc, no cudaFree, no allocating library call. */
+ * compiled into the library; grids whose face fluxes do not fit (beyond about
+ * 64^3 cells in FP64) are rejected with NS_ERR_INVALID_ARG.  The array is
+ * reserved on a device when the library's device code is loaded there, which
+ * under CUDA's default lazy loading can be the first call of this entry point
+ * on that device, and stays reserved until the process exits: make one call
+ * at start-up (or set CUDA_MODULE_LOADING=EAGER) so that no later call can
+ * fail for want of memory, and make that first call before any stream capture
+ * begins.  Every call looks up the array's address in the current context.
+ * All calls on a device share the array: calls that overlap on the GPU race,
+ * so serialise them.  Nothing is allocated: no cudaMalloc, no cudaFree, no
+ * allocating library call. */
 #define NS_NOALLOC_SCRATCH_BYTES (32u << 20)
 NS_API ns_status ns_convection_solve_noalloc(const ns_params* p, const double* W, const double* U,
                                              double* R, void* cuda_stream);

@@ -12,7 +12,7 @@
  * AoS [i][j][k][q] with 3 ghost cells per side.  Every floating-point
  * expression keeps the reference's operation order, so a build with
  * -O2 -fno-fast-math -ffp-contract=off agrees bit-for-bit with the reference
- * compiled the same way (pinned by tests/test_oracle_pin.py against the
+ * compiled the same way (pinned by tests/test_oracle_golden.py against the
  * reference build in oracle/_ref and the fixtures in tests/golden/).
  *
  * NS_SEM_PHYSICAL switches each non-textbook term of the reference to the

@@ -158,13 +158,14 @@ def ref_run(p, W, nsteps):
     return raw[:n].reshape(halo_shape(p)), raw[n:].reshape(halo_shape(p)), dts
 
 
-def ref_bench(p, steps, warmup=1, threads=None, timed=True):
-    """Times the reference's TimeScheme::step on a synthetic shear layer; returns the JSON dict."""
+def ref_bench(p, steps, warmup=1, threads=None, timed=True, ic="shear"):
+    """Times the reference's TimeScheme::step on a synthetic shear layer (ic="shear") or
+    Taylor-Green vortex (ic="tgv"); returns the JSON dict."""
     import json
     exe = REF_TIMED if timed else REF_STRICT
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
-    out = subprocess.run([exe, "bench", "in=shear", f"steps={steps}", f"warmup={warmup}"]
+    out = subprocess.run([exe, "bench", f"in={ic}", f"steps={steps}", f"warmup={warmup}"]
                          + _ref_args(p), check=True, capture_output=True, text=True, env=env)
     return json.loads(out.stdout.strip().splitlines()[-1])

@@ -2,7 +2,7 @@
 // reference tree by oracle/Makefile into oracle/_ref/) on one rank through the
 // single-rank MPI stand-in in oracle/ref_shim/mpi.h.
 //
-// TEST INFRASTRUCTURE ONLY: pins the oracle restatement (tests/test_oracle_pin.py,
+// TEST INFRASTRUCTURE ONLY: pins the oracle restatement (tests/test_oracle_golden.py,
 // tests/golden/make_golden.py) and times the reference CPU path for
 // bench.py --impl reference.  It replaces Driver::run (src/driver.cpp:3-72):
 // parameters come from the command line instead of input.xml, and the
@@ -16,7 +16,8 @@
 //                to out=, and the per-step dt to out=.dt
 //   MODE dt    : TimeScheme::set_dt on the input W; prints the dt
 //   MODE bench : steps= timed TimeScheme::step calls after warmup= untimed ones on
-//                a synthetic shear layer (in= optional); prints one JSON line
+//                a synthetic shear layer (in=shear, the default), Taylor-Green
+//                vortex (in=tgv) or a raw file; prints one JSON line
 //   MODE ic    : case= one of the test cases Driver::set_initial_condition
 //                dispatches (src/driver.cpp:107-141), set by the reference's own
 //                testcases.cpp on the zero-initialised Domain; writes W (halo'd AoS)
@@ -97,6 +98,28 @@ static void shear_layer(Array4d& W, const Params& p) {
             }
 }
 
+// Compressible Taylor-Green vortex on [0,2pi]^3 (M = 0.1) with seeded velocity
+// noise 1e-4, the same field as 3dnssolver_b200/workloads.py taylor_green
+// (SplitMix64 stream 5, three draws per cell in i-j-k order)
+static void taylor_green(Array4d& W, const Params& p) {
+    const double dx = p.Lx / p.nx, dy = p.Ly / p.ny, dz = p.Lz / p.nz, M = 0.1;
+    sm_state = 5;
+    for (int i = 0; i < p.nx; i++)
+        for (int j = 0; j < p.ny; j++)
+            for (int k = 0; k < p.nz; k++) {
+                double x = dx * 0.5 + i * dx, y = dy * 0.5 + j * dy, z = dz * 0.5 + k * dz;
+                double n0 = 1e-4 * (2.0 * sm_uniform() - 1.0);
+                double n1 = 1e-4 * (2.0 * sm_uniform() - 1.0);
+                double n2 = 1e-4 * (2.0 * sm_uniform() - 1.0);
+                W(i + 3, j + 3, k + 3, 0) = 1.0;
+                W(i + 3, j + 3, k + 3, 1) = 1.0 / (p.gamma * M * M) +
+                                            (std::cos(2 * x) + std::cos(2 * y)) * (std::cos(2 * z) + 2.0) / 16.0;
+                W(i + 3, j + 3, k + 3, 2) = std::sin(x) * std::cos(y) * std::cos(z) + n0;
+                W(i + 3, j + 3, k + 3, 3) = -std::cos(x) * std::sin(y) * std::cos(z) + n1;
+                W(i + 3, j + 3, k + 3, 4) = n2;
+            }
+}
+
 int main(int argc, char** argv) {
     if (argc < 2) {
         fprintf(stderr, "usage: ref_harness rhs|step|dt|bench key=value...\n");
@@ -174,7 +197,9 @@ int main(int argc, char** argv) {
     }
 
     std::string in = S("in", "");
-    if (!in.empty() && in != "shear") {
+    if (in == "tgv") {
+        taylor_green(W, p);
+    } else if (!in.empty() && in != "shear") {
         FILE* f = fopen(in.c_str(), "rb");
         if (!f || fread(&W(0, 0, 0, 0), sizeof(double), nall, f) != nall) {
             fprintf(stderr, "cannot read %s\n", in.c_str());

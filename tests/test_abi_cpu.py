@@ -69,7 +69,7 @@ def test_params_default_and_host_elems():
 
 @pytest.mark.parametrize("field,value", [
     ("nx", 2), ("dim", 4), ("diffusion_order", 3), ("gamma", 1.0), ("cfl", 0.0),
-    ("convection", 7), ("precision", 3), ("semantics", 5), ("Lx", -1.0),
+    ("convection", 7), ("precision", 3), ("semantics", 5), ("Lx", -1.0), ("check_finite", 2),
 ])
 def test_invalid_params_rejected_before_device_work(field, value):
     p = pkg.make_params(8, 8, 8)
@@ -96,3 +96,20 @@ def test_no_device_is_reported_not_crashed():
     with pytest.raises(pkg.NsError) as e:
         pkg.Solver(pkg.make_params(8, 8, 8))
     assert e.value.status == 7
+
+
+def test_host_buffers_of_the_wrong_shape_or_type_are_refused_on_the_host():
+    """Fault injection on the host: the C ABI takes plain pointers, so the binding refuses
+    undersized, mistyped or strided host buffers before any call crosses it."""
+    shape = pkg.halo_shape(pkg.make_params(8, 6, 4))
+    good = np.zeros(shape)
+    assert pkg.check_host_array(good, shape) is good
+    for bad in (np.zeros(shape[:-1] + (4,)), np.zeros(shape, dtype=np.float32),
+                np.zeros((shape[0] - 1,) + shape[1:]), np.zeros(shape)[:, :, ::-1],
+                np.zeros(int(np.prod(shape)))):
+        with pytest.raises(ValueError):
+            pkg.check_host_array(bad, shape)
+    ro = np.zeros(shape)
+    ro.flags.writeable = False
+    with pytest.raises(ValueError):
+        pkg.check_host_array(ro, shape, writable=True)

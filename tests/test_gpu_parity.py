@@ -236,15 +236,16 @@ def test_physical_semantics_steps_match_oracle(oracle):
     _assert_close(Ug, Uo, what="U (physical semantics)")
 
 
+@pytest.mark.parametrize("sem", [pkg.SEM_REFERENCE, pkg.SEM_PHYSICAL])
 @pytest.mark.parametrize("conv,order,bc,weights,dim", [
     (1, 2, (P, P, P), 0, 3), (2, 4, (N, P, P), 0, 3), (2, 6, (N, N, N), 1, 3), (2, 2, (P, N, P), 0, 2),
 ])
-def test_fp32_fused_stage_matches_fp32_unfused(conv, order, bc, weights, dim):
-    """The fused FP32 stage kernel (reference semantics) keeps FP32 accuracy against
-    the FP64 path (unfused kernels) on every boundary type, CD order and 2D."""
+def test_fp32_fused_stage_matches_fp32_unfused(conv, order, bc, weights, dim, sem):
+    """The fused FP32 stage kernel keeps FP32 accuracy against the FP64 path (unfused
+    kernels) on every boundary type, CD order and 2D, in both semantics."""
     shape = (20, 18, 16) if dim == 3 else (20, 18, 1)
     kw = dict(dim=dim, convection=conv, diffusion_order=order, bc=bc, weights=weights, mu=0.02,
-              cfl=0.3, precision=pkg.PREC_FP32)
+              cfl=0.3, precision=pkg.PREC_FP32, semantics=sem)
     p = pkg.make_params(*shape, **kw)
     W0 = wl.random_field(p, seed=13, smooth=False)
     with pkg.Solver(p) as s:
@@ -259,3 +260,30 @@ def test_fp32_fused_stage_matches_fp32_unfused(conv, order, bc, weights, dim):
         U64 = s.download_conservative()
     err = rel_l2(interior(Uf), interior(U64))
     assert (err[[0, 1]] <= 2e-6).all(), err
+
+
+def test_taylor_green_physical_fp64_and_fp32_match_the_oracle(oracle):
+    """The headline workload's initial condition and semantics at 24^3: the FP64 path
+    against the oracle's physical-semantics restatement (1e-12), the fused FP32 form
+    against it at FP32 accuracy, and the kinetic energy decaying as it must."""
+    import math
+    kw = dict(L=(2 * math.pi,) * 3, mu=1.0 / 1600.0, Pr=0.72, cfl=0.5, convection=pkg.CONV_WENO5_CHAR,
+              diffusion_order=2, semantics=pkg.SEM_PHYSICAL)
+    p = pkg.make_params(24, 24, 24, **kw)
+    W0 = wl.taylor_green(p)
+    Wo, Uo, dto = oracle.run(p, W0, 3)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        k0 = s.diagnostics()["kinetic"]
+        s.advance(3)
+        U64 = s.download_conservative()
+        d = s.diagnostics()
+    _assert_close(U64, Uo, what="TGV FP64 physical")
+    np.testing.assert_allclose(d["time"], dto.sum(), rtol=1e-13)
+    assert d["kinetic"] < k0
+    with pkg.Solver(pkg.make_params(24, 24, 24, precision=pkg.PREC_FP32, **kw)) as s:
+        s.upload_primitive(W0)
+        s.advance(3)
+        U32 = s.download_conservative()
+    err = rel_l2(interior(U32), interior(Uo))
+    assert (err[[0, 1]] <= 1e-6).all(), err

@@ -5,12 +5,11 @@ component-wise method on a shock problem."""
 import importlib
 import json
 import math
-import os
 
 import numpy as np
 import pytest
 
-from conftest import ROOT, interior, rel_l2
+from conftest import interior, rel_l2
 from oracle import sensor_mlp as SM
 
 pkg = importlib.import_module("3dnssolver_b200")
@@ -149,7 +148,7 @@ def test_training_learns_the_labels():
 
 
 @pytest.mark.gpu
-def test_gated_form_gains_over_component_wise():
+def test_gated_form_gains_over_component_wise(tmp_path):
     """Train on a Sod run at one resolution, gate the FP32 characteristic scheme on
     another; errors in rho and rhoE against the FP64 characteristic run."""
     import torch
@@ -184,9 +183,7 @@ def test_gated_form_gains_over_component_wise():
                      "sensor_fraction": d["sensor_fraction"]}
     res["train"] = {"faces": n, "positive_fraction": npos / n, "epoch_loss": [float(x) for x in losses]}
     print(json.dumps(res))
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "sensor_gain.json"), "w") as fh:
-        json.dump(res, fh, indent=1)
+    (tmp_path / "sensor_gain.json").write_text(json.dumps(res, indent=1))
     g, c, x = res["fp32_gated"], res["fp32_comp"], res["fp32_char"]
     assert 0.0 < g["sensor_fraction"] < 1.0
     assert g["rel_l2_rho"] < c["rel_l2_rho"] and g["rel_l2_rhoE"] < c["rel_l2_rhoE"], res
