@@ -20,7 +20,8 @@ NS_ERR_NO_DEVICE = 7
 CONV_NONE, CONV_WENO5, CONV_WENO5_CHAR = 0, 1, 2
 WEIGHTS_SHU, WEIGHTS_BORGES = 0, 1
 DIFF_NONE, DIFF_CENTERED = 0, 1
-BC_PERIODIC, BC_NEUMANN = 0, 1
+BC_PERIODIC, BC_NEUMANN, BC_EXTERNAL = 0, 1, 2
+EXCHANGE_DT, EXCHANGE_HALO = 0, 1
 PREC_FP64, PREC_FP32 = 0, 1
 SEM_REFERENCE, SEM_PHYSICAL = 0, 1
 TERM_CONVECTION, TERM_DIFFUSION, TERM_ALL = 1, 2, 3
@@ -51,7 +52,10 @@ class NsParams(ctypes.Structure):
         ("sensor", ctypes.c_int),
         ("sensor_threshold", ctypes.c_double),
         ("check_finite", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("slab_x0", ctypes.c_int),
+        ("slab_nx", ctypes.c_int),
+        ("slab_periodic", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -77,7 +81,9 @@ def make_params(nx, ny, nz, *, dim=3, L=(1.0, 1.0, 1.0), mu=1e-3, Pr=0.72, gamma
                 convection=CONV_WENO5, weights=WEIGHTS_SHU, diffusion=DIFF_CENTERED,
                 diffusion_order=2, bc=(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC),
                 precision=PREC_FP64, semantics=SEM_REFERENCE, sensor=0, sensor_threshold=0.5,
-                check_finite=0):
+                check_finite=0, slab=None):
+    """slab = (x0, nx_global, periodic): this context is the slab of cells x0..x0+nx-1 of a
+    domain of nx_global cells along x split across ranks (bc[0] becomes BC_EXTERNAL)."""
     p = NsParams()
     p.dim, p.nx, p.ny, p.nz = dim, nx, ny, nz
     p.Lx, p.Ly, p.Lz = L
@@ -89,6 +95,9 @@ def make_params(nx, ny, nz, *, dim=3, L=(1.0, 1.0, 1.0), mu=1e-3, Pr=0.72, gamma
     p.precision, p.semantics = precision, semantics
     p.sensor, p.sensor_threshold = sensor, sensor_threshold
     p.check_finite = check_finite
+    if slab is not None:
+        p.bc[0] = BC_EXTERNAL
+        p.slab_x0, p.slab_nx, p.slab_periodic = int(slab[0]), int(slab[1]), int(bool(slab[2]))
     return p
 
 

@@ -76,6 +76,12 @@ struct ns_ctx {
     long long launches = 0;
     nsb::SensorState* sensor = nullptr;
     double last_sensor_fraction = 0.0;
+    // slab decomposition: the exchange callback and, while it runs, what it exchanges
+    ns_exchange_fn xfn = nullptr;
+    void* xuser = nullptr;
+    int xwhat = -1;
+    double* xbuf = nullptr;                  // the stage input whose ghost planes are exchanged
+    unsigned long long* xslot = nullptr;     // the CFL minimum reduced over the slabs
 };
 
 static size_t host_elems(const ns_params* p) {
@@ -105,8 +111,17 @@ static ns_status validate(const ns_params* p) {
     if (p->diffusion_order != 2 && p->diffusion_order != 4 && p->diffusion_order != 6)
         return fail(NS_ERR_INVALID_ARG, "diffusion order must be 2, 4 or 6 (got %d)", p->diffusion_order);
     for (int a = 0; a < 3; a++)
-        if (p->bc[a] != NS_BC_PERIODIC && p->bc[a] != NS_BC_NEUMANN)
-            return fail(NS_ERR_INVALID_ARG, "unknown boundary type %d on axis %d", p->bc[a], a);
+        if (p->bc[a] != NS_BC_PERIODIC && p->bc[a] != NS_BC_NEUMANN && !(a == 0 && p->bc[a] == NS_BC_EXTERNAL))
+            return fail(NS_ERR_INVALID_ARG, "unknown boundary type %d on axis %d%s", p->bc[a], a,
+                        p->bc[a] == NS_BC_EXTERNAL ? " (NS_BC_EXTERNAL is for the x axis only)" : "");
+    if (p->bc[0] == NS_BC_EXTERNAL) {
+        if (p->slab_nx < p->nx || p->slab_x0 < 0 || (long long)p->slab_x0 + p->nx > p->slab_nx)
+            return fail(NS_ERR_INVALID_ARG, "slab x0 = %d, nx = %d does not lie inside a domain of %d cells",
+                        p->slab_x0, p->nx, p->slab_nx);
+        if (p->slab_periodic != 0 && p->slab_periodic != 1)
+            return fail(NS_ERR_INVALID_ARG, "slab_periodic must be 0 or 1");
+        if (p->sensor) return fail(NS_ERR_INVALID_ARG, "the sensor-gated form runs on a single domain");
+    }
     if (p->precision != NS_PREC_FP64 && p->precision != NS_PREC_FP32)
         return fail(NS_ERR_INVALID_ARG, "unknown precision %d", p->precision);
     if (p->semantics != NS_SEM_REFERENCE && p->semantics != NS_SEM_PHYSICAL)
@@ -148,6 +163,10 @@ static Consts make_consts(const ns_params* p) {
     c.inv_dz = 1.0 / c.dz;
     c.cfl = p->cfl;
     for (int a = 0; a < 3; a++) c.periodic[a] = (p->bc[a] == NS_BC_PERIODIC);
+    c.ext_x = p->bc[0] == NS_BC_EXTERNAL;
+    c.x0 = c.ext_x ? p->slab_x0 : 0;
+    c.nxg = c.ext_x ? p->slab_nx : p->nx;
+    c.xper = c.ext_x ? p->slab_periodic : c.periodic[0];
     c.dim = p->dim;
     c.order = p->diffusion_order;
     const double *df = cd2_df, *ddf = cd2_ddf;
@@ -205,6 +224,25 @@ static ns_status download(ns_ctx* ctx, const double* dev, double* host) {
 }
 
 static bool phys(const ns_ctx* ctx) { return ctx->p.semantics == NS_SEM_PHYSICAL; }
+static bool slab(const ns_ctx* ctx) { return ctx->p.bc[0] == NS_BC_EXTERNAL; }
+
+// Slab decomposition: hands the step to the exchange callback (halo planes of the
+// stage input `buf`, or the CFL minimum `slot`); nothing to do on a single domain.
+static ns_status exchange(ns_ctx* ctx, int what, double* buf, unsigned long long* slot) {
+    if (!slab(ctx)) return NS_OK;
+    if (!ctx->xfn) return fail(NS_ERR_INVALID_ARG, "a slab context (bc[0] = NS_BC_EXTERNAL) steps only with an "
+                                                   "exchange callback (ns_set_exchange)");
+    ctx->xwhat = what;
+    ctx->xbuf = buf;
+    ctx->xslot = slot;
+    g_err.clear();
+    ns_status st = ctx->xfn(ctx->xuser, ctx, what, (void*)ctx->stream);
+    ctx->xwhat = -1;
+    ctx->xbuf = nullptr;
+    ctx->xslot = nullptr;
+    if (st != NS_OK && g_err.empty()) return fail(st, "the exchange callback failed (%s)", what ? "halo" : "dt");
+    return st;
+}
 static bool fp32(const ns_ctx* ctx) { return ctx->p.precision == NS_PREC_FP32; }
 
 // optional event trail for ns_profile_step: an event after every kernel, tagged
@@ -314,9 +352,11 @@ static ns_status do_step_fused(ns_ctx* ctx) {
     const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
     const double m2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
     const double mc[3] = {-1.0, -(1. / 4.), -(2. / 3.)};
-    const double* in[3] = {ctx->U0, ctx->U, ctx->U2};
+    double* in[3] = {ctx->U0, ctx->U, ctx->U2};
     double* out[3] = {ctx->U, ctx->U2, ctx->U};
+    NS_TRY(exchange(ctx, NS_EXCHANGE_DT, nullptr, cur));
     for (int st = 0; st < 3; st++) {
+        NS_TRY(exchange(ctx, NS_EXCHANGE_HALO, in[st], nullptr));
         a.Uin = in[st];
         a.Uout = out[st];
         a.m1 = m1[st];
@@ -352,7 +392,9 @@ static ns_status do_step(ns_ctx* ctx) {
         launch_step_begin(!ctx->w_valid, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s);
         NS_TRY(check_launch(ctx, 1));
         prof_mark(ctx, NS_PROF_STEP_BEGIN);
+        NS_TRY(exchange(ctx, NS_EXCHANGE_DT, nullptr, cur));
         for (int st = 0; st < 3; st++) {
+            NS_TRY(exchange(ctx, NS_EXCHANGE_HALO, ctx->U, nullptr));
             launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
             NS_TRY(check_launch(ctx, 1));
             prof_mark(ctx, NS_PROF_FILL);
@@ -393,7 +435,9 @@ static ns_status do_step(ns_ctx* ctx) {
     // each stage); the fill then covers the halos only.  A first stage without
     // that output (after a state change or a download of W) fills all cells.
     const bool w_ready = ctx->fused_ready && ctx->w_next_ready;
+    NS_TRY(exchange(ctx, NS_EXCHANGE_DT, nullptr, cur));
     for (int st = 0; st < 3; st++) {
+        NS_TRY(exchange(ctx, NS_EXCHANGE_HALO, in[st], nullptr));
         if (st == 0 && !w_ready)
             launch_fill_prim(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
         else
@@ -866,6 +910,40 @@ ns_status ns_set_sensor_weights(ns_ctx* ctx, const float* w) {
     if (!ctx->sensor) return fail(NS_ERR_INVALID_ARG, "the context was created without the sensor (params.sensor = 0)");
     if (sensor_set_weights(ctx->sensor, w, ctx->stream) != NS_OK)
         return fail(NS_ERR_CUDA, "uploading the sensor weights failed");
+    return NS_OK;
+}
+
+ns_status ns_set_exchange(ns_ctx* ctx, ns_exchange_fn fn, void* user) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    if (!slab(ctx)) return fail(NS_ERR_INVALID_ARG, "the context is not a slab (bc[0] != NS_BC_EXTERNAL)");
+    ctx->xfn = fn;
+    ctx->xuser = user;
+    return NS_OK;
+}
+
+size_t ns_slab_elems(ns_ctx* ctx) { return ctx ? (size_t)15 * ctx->p.ny * ctx->p.nz : 0; }
+
+ns_status ns_slab_pack(ns_ctx* ctx, int side, void* buf) {
+    if (!ctx || !buf || (side != 0 && side != 1)) return fail(NS_ERR_INVALID_ARG, "ctx, side or buffer invalid");
+    if (ctx->xwhat != NS_EXCHANGE_HALO || !ctx->xbuf)
+        return fail(NS_ERR_INVALID_ARG, "ns_slab_pack is valid inside the NS_EXCHANGE_HALO callback only");
+    launch_slab_pack(ctx->xbuf, ctx->box, side, (double*)buf, ctx->stream);
+    return check_launch(ctx, 1);
+}
+
+ns_status ns_slab_unpack(ns_ctx* ctx, int side, const void* buf) {
+    if (!ctx || !buf || (side != 0 && side != 1)) return fail(NS_ERR_INVALID_ARG, "ctx, side or buffer invalid");
+    if (ctx->xwhat != NS_EXCHANGE_HALO || !ctx->xbuf)
+        return fail(NS_ERR_INVALID_ARG, "ns_slab_unpack is valid inside the NS_EXCHANGE_HALO callback only");
+    launch_slab_unpack(ctx->xbuf, ctx->box, side, (const double*)buf, ctx->stream);
+    return check_launch(ctx, 1);
+}
+
+ns_status ns_slab_dt_slot(ns_ctx* ctx, void** ptr) {
+    if (!ctx || !ptr) return fail(NS_ERR_INVALID_ARG, "ctx or ptr is NULL");
+    if (ctx->xwhat != NS_EXCHANGE_DT || !ctx->xslot)
+        return fail(NS_ERR_INVALID_ARG, "ns_slab_dt_slot is valid inside the NS_EXCHANGE_DT callback only");
+    *ptr = ctx->xslot;
     return NS_OK;
 }
 

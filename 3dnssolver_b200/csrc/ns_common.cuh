@@ -72,6 +72,10 @@ struct Consts {
     int dim;
     int order;                  // CD order 2/4/6
     double df[7], ddf[7];       // CD coefficients, centred at index 3
+    // slab of a domain split along x (NS_BC_EXTERNAL): the x ghost planes hold the
+    // neighbouring slabs' cells; x0 = global index of interior cell 0, nxg = global
+    // cells along x, xper = global x axis periodic
+    int ext_x, x0, nxg, xper;
 };
 
 #ifdef __CUDACC__
@@ -92,6 +96,32 @@ NS_HOST_DEVICE int fold(int i, int n, int periodic) {
         return r < 0 ? r + n : r;
     }
     return i < 0 ? 0 : n - 1;
+}
+
+// x index of a stencil cell outside the interior along x: folded like fold() on
+// a single domain; on a slab the ghost planes hold the neighbours' cells (or the
+// Neumann copy at a global end), so the index is used as it is.
+NS_HOST_DEVICE int fold_x(int i, int nx, const Consts& c) {
+    return c.ext_x ? i : fold(i, nx, c.periodic[0]);
+}
+
+// Whether column i (interior coordinate) lies inside the global domain along x or
+// the global x axis is periodic: the reference's derivative ghost cells are zero
+// outside (centered_diffusion.cpp:22-24 fills them only by communication).
+NS_HOST_DEVICE bool x_inside(int i, int nx, const Consts& c) {
+    if (c.ext_x) {
+        const int g = i + c.x0;
+        return (g >= 0 && g < c.nxg) || c.xper;
+    }
+    return (i >= 0 && i < nx) || c.periodic[0];
+}
+
+// Whether the lower (hi = 0) or upper (hi = 1) x ghost planes of a slab come from
+// a neighbour (exchanged) rather than from this slab's own Neumann copy.
+NS_HOST_DEVICE bool x_exchanged(int hi, int nx, const Consts& c) {
+    if (!c.ext_x) return false;
+    if (c.xper) return true;
+    return hi ? (c.x0 + nx < c.nxg) : (c.x0 > 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -177,7 +177,7 @@ __device__ __forceinline__ void march_viscous(PlaneFn plane, int i, int cc, cons
                 sxy += dx * cy1[s];
             }
             int ii = gi + s - H;
-            if ((ii >= 0 && ii < nx) || c.periodic[0]) {
+            if (x_inside(ii, nx, c)) {
                 T dy = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * H; t++)
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     // U_in of plane i at folded positions, into S without waiting (each thread
     // later converts exactly the elements it copied, so S needs no barrier)
     auto issue_plane = [&](int i) {
-        const int gi = fold(i, b.nx, c.periodic[0]);
+        const int gi = fold_x(i, b.nx, c);
         for (int e = rotated(tid, 5); e < M::NP; e += FT) {
             int py = e / M::PZ, pz = e % M::PZ;
             int gj = fold(j0 - 3 + py, b.ny, c.periodic[1]);

@@ -132,6 +132,9 @@ __global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, doubl
     if (kh >= b.nz + 2 * NG || jh >= b.NY) return;
     int i = ih - NG, j = jh - NG, k = kh - NG;
     bool ox = i < 0 || i >= b.nx, oy = j < 0 || j >= b.ny, oz = k < 0 || k >= b.nz;
+    // a slab's exchanged x ghost plane holds a neighbour's cells: its y and z ghost
+    // rows fold within the plane like those of an interior plane
+    if (ox && x_exchanged(i >= b.nx, b.nx, c)) ox = false;
     long long o = b.at(ih, jh, kh);
     double u[5], w[5];
     if ((int)ox + (int)oy + (int)oz == 1) {
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, doubl
     } else {
 #pragma unroll
         for (int q = 0; q < 5; q++) u[q] = U[q * b.fstride + o];
-        if (Uhalo && (ox || oy || oz)) {  // edges and corners travel unchanged as well
+        if (Uhalo && (i < 0 || i >= b.nx || oy || oz)) {  // edges, corners, exchanged planes travel unchanged
 #pragma unroll
             for (int q = 0; q < 5; q++) Uhalo[q * b.fstride + o] = u[q];
         }
@@ -166,30 +169,43 @@ __global__ void __launch_bounds__(128) k_fill_halo(double* __restrict__ W, doubl
                                                    Box b, Consts c, double* __restrict__ Uhalo) {
     const int ax = blockIdx.y >> 1, hi = blockIdx.y & 1;
     const long long t = (long long)blockIdx.x * 128 + threadIdx.x;
+    // on a slab the y and z ghost rows of exchanged x ghost planes are filled too
+    const int ilo = x_exchanged(0, b.nx, c) ? -NG : 0, ihi = b.nx + (x_exchanged(1, b.nx, c) ? NG : 0);
+    const int nxe = ihi - ilo;
     int i, j, k, layer;
     if (ax == 0) {
         if (t >= 3LL * b.ny * b.nz) return;
         k = (int)(t % b.nz); j = (int)((t / b.nz) % b.ny); layer = (int)(t / ((long long)b.nz * b.ny));
         i = hi ? b.nx + layer : layer - NG;
     } else if (ax == 1) {
-        if (t >= 3LL * b.nx * b.nz) return;
-        k = (int)(t % b.nz); i = (int)((t / b.nz) % b.nx); layer = (int)(t / ((long long)b.nz * b.nx));
+        if (t >= 3LL * nxe * b.nz) return;
+        k = (int)(t % b.nz); i = ilo + (int)((t / b.nz) % nxe); layer = (int)(t / ((long long)b.nz * nxe));
         j = hi ? b.ny + layer : layer - NG;
     } else {
-        if (t >= 3LL * b.nx * b.ny) return;
-        layer = (int)(t % 3); j = (int)((t / 3) % b.ny); i = (int)(t / (3LL * b.ny));
+        if (t >= 3LL * nxe * b.ny) return;
+        layer = (int)(t % 3); j = (int)((t / 3) % b.ny); i = ilo + (int)(t / (3LL * b.ny));
         k = hi ? b.nz + layer : layer - NG;
     }
-    const int si = ax == 0 ? fold(i, b.nx, c.periodic[0]) : i;
-    const int sj = ax == 1 ? fold(j, b.ny, c.periodic[1]) : j;
-    const int sk = ax == 2 ? fold(k, b.nz, c.periodic[2]) : k;
-    const long long o = b.at(i + NG, j + NG, k + NG), src = b.at(si + NG, sj + NG, sk + NG);
+    const long long o = b.at(i + NG, j + NG, k + NG);
     double u[5], w[5];
+    if (ax == 0 && x_exchanged(hi, b.nx, c)) {
+        // a neighbour's cells, already in place
 #pragma unroll
-    for (int q = 0; q < 5; q++) {
-        u[q] = U[q * b.fstride + src];
-        U[q * b.fstride + o] = u[q];
-        if (Uhalo) Uhalo[q * b.fstride + o] = u[q];
+        for (int q = 0; q < 5; q++) {
+            u[q] = U[q * b.fstride + o];
+            if (Uhalo) Uhalo[q * b.fstride + o] = u[q];
+        }
+    } else {
+        const int si = ax == 0 ? fold(i, b.nx, c.periodic[0]) : i;
+        const int sj = ax == 1 ? fold(j, b.ny, c.periodic[1]) : j;
+        const int sk = ax == 2 ? fold(k, b.nz, c.periodic[2]) : k;
+        const long long src = b.at(si + NG, sj + NG, sk + NG);
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            u[q] = U[q * b.fstride + src];
+            U[q * b.fstride + o] = u[q];
+            if (Uhalo) Uhalo[q * b.fstride + o] = u[q];
+        }
     }
     prim_from_cons(u, c.gm1, w);
 #pragma unroll
@@ -346,13 +362,13 @@ __device__ __forceinline__ void viscous_reference(const double* __restrict__ W, 
             // d/dx of (d/dy W) at column i+s-H
             const int ii = i + s - H;
             {
-                const int iw = fold(ii, b.nx, 1);
+                const int iw = c.ext_x ? ii : fold(ii, b.nx, 1);
                 const long long ob = b.at(iw + NG, j + NG, k + NG);
                 TV dy = 0;
 #pragma unroll
                 for (int t = 0; t <= 2 * H; t++)
                     if (t != H) dy += TV(W[q * fs + ob + (t - H) * sy]) * cy1[t];
-                if ((ii >= 0 && ii < b.nx) || c.periodic[0]) syx += dy * cx1[s];
+                if (x_inside(ii, b.nx, c)) syx += dy * cx1[s];
             }
         }
         Dxy[v] = sxy; Dyx[v] = syx;
@@ -404,9 +420,10 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
                     int cc[3] = {c3[0], c3[1], c3[2]};
                     cc[a] += s - H;
                     cc[bx] += t - H;
-                    // corner/edge cells are not filled: fold along both axes
-                    cc[a] = fold(cc[a], n3[a], c.periodic[a]);
-                    cc[bx] = fold(cc[bx], n3[bx], c.periodic[bx]);
+                    // corner/edge cells are not filled: fold along both axes (a slab's
+                    // x ghost planes are the neighbours' cells and stay as they are)
+                    if (a != 0 || !c.ext_x) cc[a] = fold(cc[a], n3[a], c.periodic[a]);
+                    if (bx != 0 || !c.ext_x) cc[bx] = fold(cc[bx], n3[bx], c.periodic[bx]);
                     long long oo = b.at(cc[0] + NG, cc[1] + NG, cc[2] + NG);
                     acc += TV(W[(2 + bx) * fs + oo]) * TV(c.df[3 - H + s] * inv[a]) *
                            TV(c.df[3 - H + t] * inv[bx]);
@@ -692,6 +709,33 @@ __global__ void __launch_bounds__(128) k_soa_to_aos(const double* __restrict__ S
 }
 
 // ---------------------------------------------------------------------------
+// slab halo exchange (Communicator::communicate_x_direction, src/communicator.cpp:16-57,
+// with the slices of src/containers/array_4d.cpp:39-84): the outer three interior
+// planes of one side packed as [q][layer][j][k], interior j and k; unpack writes
+// the same layout into the ghost planes of that side.
+__global__ void __launch_bounds__(128) k_slab_pack(const double* __restrict__ U, Box b, int side,
+                                                   double* __restrict__ buf) {
+    const long long n = 3LL * b.ny * b.nz, t = (long long)blockIdx.x * 128 + threadIdx.x;
+    if (t >= 5 * n) return;
+    const int q = (int)(t / n);
+    const long long r = t % n;
+    const int layer = (int)(r / ((long long)b.ny * b.nz)), j = (int)((r / b.nz) % b.ny), k = (int)(r % b.nz);
+    const int i = side ? b.nx - NG + layer : layer;
+    buf[t] = U[q * b.fstride + b.at(i + NG, j + NG, k + NG)];
+}
+
+__global__ void __launch_bounds__(128) k_slab_unpack(double* __restrict__ U, Box b, int side,
+                                                     const double* __restrict__ buf) {
+    const long long n = 3LL * b.ny * b.nz, t = (long long)blockIdx.x * 128 + threadIdx.x;
+    if (t >= 5 * n) return;
+    const int q = (int)(t / n);
+    const long long r = t % n;
+    const int layer = (int)(r / ((long long)b.ny * b.nz)), j = (int)((r / b.nz) % b.ny), k = (int)(r % b.nz);
+    const int i = side ? b.nx + layer : layer - NG;
+    U[q * b.fstride + b.at(i + NG, j + NG, k + NG)] = buf[t];
+}
+
+// ---------------------------------------------------------------------------
 // global diagnostics over the interior (FP64): sums of conserved variables,
 // kinetic energy, enstrophy (second-order central curl), non-finite count.
 __global__ void __launch_bounds__(128) k_diagnostics(const double* __restrict__ U, Box b, Consts c,
@@ -718,7 +762,7 @@ __global__ void __launch_bounds__(128) k_diagnostics(const double* __restrict__ 
         v[5] = 0.5 * (u[2] * u[2] + u[3] * u[3] + u[4] * u[4]) / u[0] * dV;
         // velocity of neighbours through the periodic/clamped index map
         auto vel = [&](int ii, int jj, int kk, int a) {
-            ii = fold(ii, b.nx, c.periodic[0]);
+            ii = fold_x(ii, b.nx, c);
             jj = fold(jj, b.ny, c.periodic[1]);
             kk = fold(kk, b.nz, c.periodic[2]);
             long long oo = b.at(ii + NG, jj + NG, kk + NG);
@@ -817,7 +861,8 @@ void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, un
 }
 
 void launch_fill_halo(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s, double* Uhalo) {
-    const long long area = std::max(std::max((long long)b.ny * b.nz, (long long)b.nx * b.nz), (long long)b.nx * b.ny);
+    const long long nxe = b.nx + (c.ext_x ? 2 * NG : 0);  // slabs: y/z ghost rows of the x ghost planes too
+    const long long area = std::max(std::max((long long)b.ny * b.nz, nxe * b.nz), nxe * b.ny);
     k_fill_halo<<<dim3((unsigned)((3 * area + 127) / 128), 6), 128, 0, s>>>(W, U, b, c, Uhalo);
 }
 
@@ -965,6 +1010,15 @@ void launch_check_state(const double* A, bool prim, const Box& b, const Consts& 
                         unsigned long long* count, cudaStream_t s) {
     if (prim) k_check_state<true><<<interior_grid(b), dim3(32, 4), 0, s>>>(A, b, c, count);
     else k_check_state<false><<<interior_grid(b), dim3(32, 4), 0, s>>>(A, b, c, count);
+}
+
+void launch_slab_pack(const double* U, const Box& b, int side, double* buf, cudaStream_t s) {
+    const long long n = 15LL * b.ny * b.nz;
+    k_slab_pack<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(U, b, side, buf);
+}
+void launch_slab_unpack(double* U, const Box& b, int side, const double* buf, cudaStream_t s) {
+    const long long n = 15LL * b.ny * b.nz;
+    k_slab_unpack<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(U, b, side, buf);
 }
 
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s) {

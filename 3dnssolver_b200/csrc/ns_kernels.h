@@ -87,6 +87,9 @@ void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_
 // vs >= nx ny nz), half-width h = order/2 of the centered scheme
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
                     long long vs, cudaStream_t s);
+// slab halo exchange: pack the outer interior planes of a side / unpack into its ghost planes
+void launch_slab_pack(const double* U, const Box& b, int side, double* buf, cudaStream_t s);
+void launch_slab_unpack(double* U, const Box& b, int side, const double* buf, cudaStream_t s);
 void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s);
 void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s);
 // interior cells of A (W if prim, else U) that are non-finite or have rho <= 0 or p <= 0,

@@ -55,8 +55,12 @@ enum { NS_WEIGHTS_SHU = 0, NS_WEIGHTS_BORGES = 1 };
 /* DiffusionScheme factory choices, src/driver.cpp:96-105 */
 enum { NS_DIFF_NONE = 0, NS_DIFF_CENTERED = 1 };
 /* Per-axis boundary: periodic (MPI_Cart periodic flag, src/decomposition.cpp:116-161)
- * or zeroth-order Neumann copy (src/boundary_conditions/boundary_neumann.cpp:22-132). */
-enum { NS_BC_PERIODIC = 0, NS_BC_NEUMANN = 1 };
+ * or zeroth-order Neumann copy (src/boundary_conditions/boundary_neumann.cpp:22-132).
+ * NS_BC_EXTERNAL (x axis only): the context is one slab of a domain split along x
+ * (src/decomposition.cpp:116-143, one rank per GPU); its x ghost planes are the
+ * neighbouring slabs' cells, which an exchange callback brings in before every
+ * RK stage (src/communicator.cpp:16-57), see ns_set_exchange. */
+enum { NS_BC_PERIODIC = 0, NS_BC_NEUMANN = 1, NS_BC_EXTERNAL = 2 };
 /* Arithmetic of the stencil / flux / WENO work.  FP32 keeps the RK3
  * accumulation and all global reductions in FP64. */
 enum { NS_PREC_FP64 = 0, NS_PREC_FP32 = 1 };
@@ -86,7 +90,12 @@ typedef struct ns_params {
                           * return NS_ERR_NONFINITE if an interior cell holds NaN/Inf or a
                           * non-positive density or pressure (the reference lets NaN propagate
                           * silently, src/time_scheme.cpp:104-117); 0 (default): no check */
-    int reserved[7];
+    /* slab decomposition along x (bc[0] = NS_BC_EXTERNAL): */
+    int slab_x0;         /* global index of this slab's first x cell */
+    int slab_nx;         /* global cells along x (the slabs' nx sum to it) */
+    int slab_periodic;   /* 1: the global x axis is periodic; 0: Neumann at the global ends
+                          * (the end slabs fill their outer ghost planes themselves) */
+    int reserved[4];
 } ns_params;
 
 /* Global diagnostics of the device state (no reference counterpart: the
@@ -181,6 +190,39 @@ enum { NS_PROF_STEP_BEGIN = 0, NS_PROF_FILL = 1, NS_PROF_FACE_X = 2, NS_PROF_FAC
  * of kernel class c summed over the step, for c < n (n >= 7; classes at or
  * above n are left out of ms). */
 NS_API ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n);
+/* ---- slab decomposition along x (multi-GPU) --------------------------------
+ * Replaces the MPI halo exchange and dt reduction of the reference
+ * (Communicator::communicate_x_direction, src/communicator.cpp:16-57, and the
+ * MPI_Allreduce(MIN) of TimeScheme::set_dt, src/time_scheme.cpp:127-136) for a
+ * context created with bc[0] = NS_BC_EXTERNAL.  The time-step calls
+ * (ns_advance, ns_time_step) call the exchange callback on the context's stream
+ * at two points of every step:
+ *   what = NS_EXCHANGE_DT: before the first stage; the CFL minimum of this slab
+ *     is in the 8 bytes at ns_slab_dt_slot (the bits of a positive double, or
+ *     all ones if the slab has no finite value); the callback replaces it with
+ *     the minimum over all slabs (as unsigned 64-bit integers);
+ *   what = NS_EXCHANGE_HALO: before each of the three stages; the callback packs
+ *     this slab's outer interior planes (ns_slab_pack), sends them to the
+ *     neighbouring slabs, receives theirs and unpacks them into the ghost planes
+ *     (ns_slab_unpack).  Sides at a non-periodic global end are filled by the
+ *     library (Neumann) and need no exchange.
+ * The callback enqueues all device work on the given stream (NCCL send/recv
+ * on that stream, or host-staged copies) and returns NS_OK or an error, which
+ * the step returns.  No kernel of the library waits on another slab. */
+enum { NS_EXCHANGE_DT = 0, NS_EXCHANGE_HALO = 1 };
+typedef ns_status (*ns_exchange_fn)(void* user, ns_ctx* ctx, int what, void* cuda_stream);
+NS_API ns_status ns_set_exchange(ns_ctx* ctx, ns_exchange_fn fn, void* user);
+/* Doubles of one packed side: 5 x 3 x ny x nz, order [q][layer][j][k]. */
+NS_API size_t ns_slab_elems(ns_ctx* ctx);
+/* Inside the NS_EXCHANGE_HALO callback: side 0 packs interior planes 0..2
+ * (for the lower neighbour's upper ghost planes), side 1 planes nx-3..nx-1;
+ * unpack writes ghost planes -3..-1 (side 0) or nx..nx+2 (side 1) of the
+ * stage's input state.  dev_buf: ns_slab_elems doubles of device memory. */
+NS_API ns_status ns_slab_pack(ns_ctx* ctx, int side, void* dev_buf);
+NS_API ns_status ns_slab_unpack(ns_ctx* ctx, int side, const void* dev_buf);
+/* Device address of the 8-byte CFL minimum slot (inside the NS_EXCHANGE_DT callback). */
+NS_API ns_status ns_slab_dt_slot(ns_ctx* ctx, void** dev_ptr);
+
 /* ---- learned troubled-face sensor (no reference counterpart) ----------------
  * An MLP 21 -> 32 -> 32 -> 1 (GELU) predicts from a face's stencil whether the
  * characteristic-wise WENO-5 flux differs from the component-wise one by more

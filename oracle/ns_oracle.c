@@ -30,12 +30,22 @@
 typedef struct {
     int nx, ny, nz, NX, NY, NZ;
     double dx, dy, dz;
+    /* slab of a domain split along x (bc[0] = NS_BC_EXTERNAL): whether the lower
+     * and upper x ghost planes come from a neighbour, and the x range of planes
+     * whose y/z ghost rows and y-derivatives are formed (the interior, plus
+     * exchanged ghost planes) */
+    int ext, exlo, exhi, xlo, xhi;
 } geom;
 
 static geom make_geom(const ns_params* p) {
     geom g;
     g.nx = p->nx; g.ny = p->ny; g.nz = p->nz;
     g.NX = p->nx + 2 * NG; g.NY = p->ny + 2 * NG; g.NZ = p->nz + 2 * NG;
+    g.ext = p->bc[0] == NS_BC_EXTERNAL;
+    g.exlo = g.ext && (p->slab_periodic || p->slab_x0 > 0);
+    g.exhi = g.ext && (p->slab_periodic || p->slab_x0 + p->nx < p->slab_nx);
+    g.xlo = g.exlo ? 0 : NG;
+    g.xhi = p->nx + NG + (g.exhi ? NG : 0);
     /* src/grid.cpp:12-19 */
     g.dx = p->Lx / p->nx; g.dy = p->Ly / p->ny; g.dz = p->Lz / p->nz;
     return g;
@@ -98,17 +108,20 @@ static void cons_to_prim(const ns_params* p, const geom* g, const double* U, dou
  * MPI_Sendrecv does. */
 
 static void neumann_fill(const ns_params* p, const geom* g, double* A) {
-    if (p->bc[0] == NS_BC_NEUMANN) {
+    /* a slab fills only the x sides at a non-periodic global end */
+    const int xlo_fill = p->bc[0] == NS_BC_NEUMANN || (g->ext && !g->exlo);
+    const int xhi_fill = p->bc[0] == NS_BC_NEUMANN || (g->ext && !g->exhi);
+    if (xlo_fill || xhi_fill) {
         for (int i = 0; i < NG; i++)
             for (int j = NG; j < g->ny + NG; j++)
                 for (int k = NG; k < g->nz + NG; k++)
                     for (int q = 0; q < NQ; q++) {
-                        A[IX(g, i, j, k, q)] = A[IX(g, NG, j, k, q)];
-                        A[IX(g, g->nx + NG + i, j, k, q)] = A[IX(g, g->nx + NG - 1, j, k, q)];
+                        if (xlo_fill) A[IX(g, i, j, k, q)] = A[IX(g, NG, j, k, q)];
+                        if (xhi_fill) A[IX(g, g->nx + NG + i, j, k, q)] = A[IX(g, g->nx + NG - 1, j, k, q)];
                     }
     }
     if (p->bc[1] == NS_BC_NEUMANN) {
-        for (int i = NG; i < g->nx + NG; i++)
+        for (int i = g->xlo; i < g->xhi; i++)
             for (int j = 0; j < NG; j++)
                 for (int k = NG; k < g->nz + NG; k++)
                     for (int q = 0; q < NQ; q++) {
@@ -117,7 +130,7 @@ static void neumann_fill(const ns_params* p, const geom* g, double* A) {
                     }
     }
     if (p->bc[2] == NS_BC_NEUMANN) {
-        for (int i = NG; i < g->nx + NG; i++)
+        for (int i = g->xlo; i < g->xhi; i++)
             for (int j = NG; j < g->ny + NG; j++)
                 for (int k = 0; k < NG; k++)
                     for (int q = 0; q < NQ; q++) {
@@ -127,15 +140,16 @@ static void neumann_fill(const ns_params* p, const geom* g, double* A) {
     }
 }
 
-/* copy the face slab [lo, lo+3) of axis `ax` to [dst, dst+3), other axes interior */
+/* copy the face slab [lo, lo+3) of axis `ax` to [dst, dst+3), other axes interior
+ * (along x: the planes xlo..xhi-1, which include a slab's exchanged ghost planes) */
 static void slab_copy(const geom* g, double* A, int ax, int src, int dst) {
-    int n0 = (ax == 0) ? NG : g->nx, n1 = (ax == 1) ? NG : g->ny, n2 = (ax == 2) ? NG : g->nz;
+    int n0 = (ax == 0) ? NG : g->xhi - g->xlo, n1 = (ax == 1) ? NG : g->ny, n2 = (ax == 2) ? NG : g->nz;
     size_t cnt = (size_t)n0 * n1 * n2 * NQ, c = 0;
     double* buf = (double*)malloc(cnt * sizeof(double));
     for (int a = 0; a < n0; a++)
         for (int b = 0; b < n1; b++)
             for (int d = 0; d < n2; d++) {
-                int i = (ax == 0) ? src + a : NG + a;
+                int i = (ax == 0) ? src + a : g->xlo + a;
                 int j = (ax == 1) ? src + b : NG + b;
                 int k = (ax == 2) ? src + d : NG + d;
                 for (int q = 0; q < NQ; q++) buf[c++] = A[IX(g, i, j, k, q)];
@@ -144,7 +158,7 @@ static void slab_copy(const geom* g, double* A, int ax, int src, int dst) {
     for (int a = 0; a < n0; a++)
         for (int b = 0; b < n1; b++)
             for (int d = 0; d < n2; d++) {
-                int i = (ax == 0) ? dst + a : NG + a;
+                int i = (ax == 0) ? dst + a : g->xlo + a;
                 int j = (ax == 1) ? dst + b : NG + b;
                 int k = (ax == 2) ? dst + d : NG + d;
                 for (int q = 0; q < NQ; q++) A[IX(g, i, j, k, q)] = buf[c++];
@@ -155,7 +169,8 @@ static void slab_copy(const geom* g, double* A, int ax, int src, int dst) {
 static void communicate(const ns_params* p, const geom* g, double* A) {
     const int n[3] = {g->nx, g->ny, g->nz};
     for (int ax = 0; ax < 3; ax++) {
-        if (p->bc[ax] != NS_BC_PERIODIC) continue; /* MPI_PROC_NULL: no-op */
+        /* MPI_PROC_NULL: no-op; a slab's x ghost planes come from the exchange */
+        if (p->bc[ax] != NS_BC_PERIODIC) continue;
         slab_copy(g, A, ax, n[ax], 0);        /* "east to east": arr(n) -> arr(0) */
         slab_copy(g, A, ax, NG, NG + n[ax]);  /* "west to west": arr(ngc) -> arr(ngc+n) */
     }
@@ -428,12 +443,13 @@ static void cd_coeffs(int order, const double** df, const double** ddf, int* w) 
     else { *df = cd2_df; *ddf = cd2_ddf; *w = 3; }
 }
 
-/* generic_fd_{x,y,z}: df = sum f(.. + start + idx ..) * c[idx] / d over interior */
-static void generic_fd(const geom* g, int ax, const double* f, double* df, const double* c,
-                       int w, double d) {
+/* generic_fd_{x,y,z}: df = sum f(.. + start + idx ..) * c[idx] / d over interior
+ * (x planes ilo..ihi-1) */
+static void generic_fd_range(const geom* g, int ax, const double* f, double* df, const double* c,
+                             int w, double d, int ilo, int ihi) {
     const int start = -(w / 2);
 #pragma omp parallel for schedule(static)
-    for (int i = NG; i < g->nx + NG; i++)
+    for (int i = ilo; i < ihi; i++)
         for (int j = NG; j < g->ny + NG; j++)
             for (int k = NG; k < g->nz + NG; k++)
                 for (int q = 0; q < NQ; q++) {
@@ -445,6 +461,11 @@ static void generic_fd(const geom* g, int ax, const double* f, double* df, const
                     }
                     df[IX(g, i, j, k, q)] = sum;
                 }
+}
+
+static void generic_fd(const geom* g, int ax, const double* f, double* df, const double* c,
+                       int w, double d) {
+    generic_fd_range(g, ax, f, df, c, w, d, NG, g->nx + NG);
 }
 
 /* DiffusionScheme stress helpers, src/diffusion_schemes/diffusion_scheme.cpp:3-58 */
@@ -492,7 +513,9 @@ static void diffusion_solve_reference(const ns_params* p, const geom* g, const d
     generic_fd(g, 0, W, Dxx, ddf, w, g->dx * g->dx);
     generic_fd(g, 0, W, Dyy, ddf, w, g->dy * g->dy); /* ddf_dydy differentiates along x (cd-n.cpp:77) */
     generic_fd(g, 0, W, Dx, df, w, g->dx);
-    generic_fd(g, 1, W, Dy, df, w, g->dy);
+    /* a slab forms dW/dy on its exchanged x ghost planes too: the neighbour's values,
+     * which the reference's communicate(dW_y) brings in across ranks */
+    generic_fd_range(g, 1, W, Dy, df, w, g->dy, g->xlo, g->xhi);
     communicate(p, g, Dx); /* centered_diffusion.cpp:22-24: only periodic halos are filled */
     communicate(p, g, Dy);
     generic_fd(g, 1, Dx, Dxy, df, w, g->dy);
@@ -618,6 +641,7 @@ static void diffusion_solve_physical(const ns_params* p, const geom* g, const do
                                     int cc[3] = {ii, jj, kk};
                                     const int nn[3] = {g->nx, g->ny, g->nz};
                                     for (int e = 0; e < 3; e++) {
+                                        if (e == 0 && g->ext) continue; /* ghost planes: the neighbours' cells */
                                         if (cc[e] < NG || cc[e] >= nn[e] + NG) {
                                             if (p->bc[e] == NS_BC_PERIODIC)
                                                 cc[e] = NG + ((cc[e] - NG) % nn[e] + nn[e]) % nn[e];
@@ -810,6 +834,48 @@ int nso_time_step(const ns_params* p, double* W, double* U, double* dt_out) {
     if (dt_out) *dt_out = dt;
     free(R); free(Uprev);
     return 0;
+}
+
+/* Slab decomposition along x (bc[0] = NS_BC_EXTERNAL): nsteps of TimeScheme::step
+ * on one slab, with the halo exchange and dt reduction of the reference's MPI
+ * path (communicator.cpp:16-57, time_scheme.cpp:127-136) delegated to fn:
+ *   fn(user, 0, &dt_min): replace the slab's CFL minimum by the minimum over slabs
+ *   fn(user, 1, U): fill U's x ghost planes (interior j, k) from the neighbours
+ * fn returns 0 on success. */
+typedef int (*nso_exchange_fn)(void* user, int what, double* data);
+
+int nso_slab_run(const ns_params* p, double* W, double* U, int nsteps, double* dts, nso_exchange_fn fn,
+                 void* user) {
+    if (check(p) || !fn) return 1;
+    geom g = make_geom(p);
+    double* R = zeros(&g);
+    double* Uprev = zeros(&g);
+    const double m1s[3] = {1.0, 3.0 / 4.0, 1. / 3.};
+    const double m2s[3] = {0.0, 1.0 / 4.0, 2. / 3.};
+    int rc = 0;
+    for (int s = 0; s < nsteps && !rc; s++) {
+        double m = local_max_dt(p, &g, W);
+        if (fn(user, 0, &m)) { rc = 2; break; }
+        double dt = m * p->cfl;
+        const double m3s[3] = {-dt, -(1. / 4.) * dt, -(2. / 3.) * dt};
+        prim_to_cons(p, &g, W, U);
+        interior_copy(&g, U, Uprev);
+        for (int st = 0; st < 3; st++) {
+            memset(R, 0, n_all(&g) * sizeof(double));
+            if (fn(user, 1, U)) { rc = 2; break; }
+            neumann_fill(p, &g, U);
+            communicate(p, &g, U);
+            cons_to_prim(p, &g, U, W);
+            convection_solve(p, &g, W, U, R);
+            diffusion_solve(p, &g, W, R);
+            substep(&g, U, Uprev, R, m1s[st], m2s[st], m3s[st]);
+        }
+        if (rc) break;
+        cons_to_prim(p, &g, U, W);
+        if (dts) dts[s] = dt;
+    }
+    free(R); free(Uprev);
+    return rc;
 }
 
 /* n steps; dts (may be NULL) receives each step's dt */

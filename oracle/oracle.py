@@ -23,6 +23,8 @@ halo_shape = _abi.halo_shape
 params_dict = _abi.params_dict
 
 _lib = None
+# int fn(void* user, int what, double* data): what 0 = dt minimum, 1 = x ghost planes of U
+SLAB_EXCHANGE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double))
 
 
 def build():
@@ -50,6 +52,8 @@ def lib():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = ctypes.c_int
+        L.nso_slab_run.argtypes = [P, dp, dp, ctypes.c_int, dp, SLAB_EXCHANGE_FN, ctypes.c_void_p]
+        L.nso_slab_run.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -113,6 +117,29 @@ def run(p, W, nsteps):
     U = np.zeros_like(W)
     dts = np.zeros(max(nsteps, 1))
     _check(lib().nso_run(ctypes.byref(p), _ptr(W), _ptr(U), nsteps, _ptr(dts)), "run")
+    return W, U, dts[:nsteps]
+
+
+def slab_run(p, W, nsteps, exchange):
+    """nsteps on one slab (bc[0] = NS_BC_EXTERNAL); exchange(what, data) fills the x ghost
+    planes of U (what = 1, data: the halo'd AoS array) or returns the minimum over slabs
+    of a CFL minimum (what = 0, data: a 1-element array it updates).  Returns (W, U, dts)."""
+    W = np.ascontiguousarray(W, dtype=np.float64).copy()
+    U = np.zeros_like(W)
+    dts = np.zeros(max(nsteps, 1))
+    shape = W.shape
+
+    def cb(user, what, data):
+        try:
+            exchange(what, np.ctypeslib.as_array(data, shape=(1,) if what == 0 else shape))
+            return 0
+        except Exception:
+            import traceback
+            traceback.print_exc()
+            return 1
+
+    fn = SLAB_EXCHANGE_FN(cb)
+    _check(lib().nso_slab_run(ctypes.byref(p), _ptr(W), _ptr(U), nsteps, _ptr(dts), fn, None), "slab_run")
     return W, U, dts[:nsteps]
 
 

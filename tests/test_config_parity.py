@@ -1,0 +1,91 @@
+"""GPU parity at the sizes of the benchmark configurations, through the C ABI,
+against the oracle (OpenMP on the host cores; the oracle is pinned bit-for-bit
+to the reference by tests/test_oracle_golden.py).
+
+  config 1: shear layer 64^3, component-wise WENO-5 + CD-2, 100 steps at CFL 0.5
+  config 2: shear layer 256^3, characteristic-wise WENO-5 + CD-2: one first-stage
+            right-hand side and one time step
+  config 3: Sod shock tube, characteristic-wise, one time step on 128x32x32 with
+            the stable setting Ly = Lz = 1 (dy = dz = 4 dx at 512x128x128; here 4 dx too)
+
+Tolerance: 1e-12 relative L2 per conserved field, as in tests/test_gpu_parity.py.
+rhoW of the shear layer is a noise-amplitude field (1e-3 seeded noise), so it is
+judged against the momentum magnitude, as two CPU builds of the reference
+already differ by 4e-12 in its own norm after 100 steps.
+"""
+import importlib
+import math
+
+import numpy as np
+import pytest
+
+from conftest import interior, rel_l2
+
+pkg = importlib.import_module("3dnssolver_b200")
+wl = importlib.import_module("3dnssolver_b200.workloads")
+sensor = importlib.import_module("3dnssolver_b200.sensor")
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+def _shear(n, conv):
+    L = 2 * math.pi
+    return pkg.make_params(n, n, n, L=(L, L, L), mu=2.0 * 0.05 * 2 * math.pi / 1000.0, Pr=0.72, cfl=0.5,
+                           convection=conv, diffusion_order=2)
+
+
+def _check(Ug, Uo, what):
+    a, b = interior(Ug), interior(Uo)
+    err = rel_l2(a, b)
+    mag = np.sqrt((b[..., 2:5] ** 2).sum())
+    err_w = np.sqrt(((a[..., 4] - b[..., 4]) ** 2).sum()) / mag
+    assert np.isfinite(a).all(), what
+    assert (err[:4] <= TOL).all(), f"{what}: rel L2 per field {err}"
+    assert err_w <= TOL, f"{what}: rhoW against the momentum magnitude {err_w}"
+    return err
+
+
+def test_config1_shear64_component_wise_100_steps(oracle):
+    p = _shear(64, pkg.CONV_WENO5)
+    W0 = wl.shear_layer(p, seed=1)
+    Wo, Uo, dto = oracle.run(p, W0, 100)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(100)
+        Ug = s.download_conservative()
+        dt, t = s.get_dt()
+    _check(Ug, Uo, "config 1 after 100 steps")
+    assert dt == pytest.approx(dto[-1], rel=1e-12)
+    assert t == pytest.approx(dto.sum(), rel=1e-12)
+
+
+def test_config2_shear256_characteristic_rhs_and_step(oracle):
+    p = _shear(256, pkg.CONV_WENO5_CHAR)
+    W0 = wl.shear_layer(p, seed=1)
+    with pkg.Solver(p) as s:
+        R = s.rhs(W0)
+        Wg, Ug = W0.copy(), s.new_array()
+        dt = s.time_step(Wg, Ug)
+    Ro = oracle.rhs(p, W0)
+    err = rel_l2(interior(R), interior(Ro))
+    assert (err <= TOL).all(), f"config 2 rhs: rel L2 per field {err}"
+    Wo, Uo, dto = oracle.run(p, W0, 1)
+    assert dt == pytest.approx(dto[0], rel=1e-14)
+    _check(Ug, Uo, "config 2 one step")
+
+
+def test_config3_sod_characteristic_one_step(oracle):
+    p = sensor.sod_params(128, 32, 32)  # Ly = Lz = 1: dy = dz = 4 dx
+    W0 = wl.sod(p, seed=3)
+    Wo, Uo, dto = oracle.run(p, W0, 1)
+    with pkg.Solver(p) as s:
+        Wg, Ug = W0.copy(), s.new_array()
+        dt = s.time_step(Wg, Ug)
+    assert dt == pytest.approx(dto[0], rel=1e-14)
+    err = rel_l2(interior(Ug), interior(Uo))
+    # rhoV and rhoW start at zero and are driven by the perturbed interface only
+    mag = np.sqrt((interior(Uo)[..., 2:5] ** 2).sum())
+    err_t = np.sqrt(((interior(Ug)[..., 3:5] - interior(Uo)[..., 3:5]) ** 2).sum((0, 1, 2))) / mag
+    assert (err[:3] <= TOL).all(), f"config 3 one step: rel L2 per field {err}"
+    assert (err_t <= TOL).all(), err_t
