@@ -55,7 +55,8 @@ class NsParams(ctypes.Structure):
         ("slab_x0", ctypes.c_int),
         ("slab_nx", ctypes.c_int),
         ("slab_periodic", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("sensor_period", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -81,7 +82,7 @@ def make_params(nx, ny, nz, *, dim=3, L=(1.0, 1.0, 1.0), mu=1e-3, Pr=0.72, gamma
                 convection=CONV_WENO5, weights=WEIGHTS_SHU, diffusion=DIFF_CENTERED,
                 diffusion_order=2, bc=(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC),
                 precision=PREC_FP64, semantics=SEM_REFERENCE, sensor=0, sensor_threshold=0.5,
-                check_finite=0, slab=None):
+                check_finite=0, slab=None, sensor_period=1):
     """slab = (x0, nx_global, periodic): this context is the slab of cells x0..x0+nx-1 of a
     domain of nx_global cells along x split across ranks (bc[0] becomes BC_EXTERNAL)."""
     p = NsParams()
@@ -95,6 +96,7 @@ def make_params(nx, ny, nz, *, dim=3, L=(1.0, 1.0, 1.0), mu=1e-3, Pr=0.72, gamma
     p.precision, p.semantics = precision, semantics
     p.sensor, p.sensor_threshold = sensor, sensor_threshold
     p.check_finite = check_finite
+    p.sensor_period = sensor_period
     if slab is not None:
         p.bc[0] = BC_EXTERNAL
         p.slab_x0, p.slab_nx, p.slab_periodic = int(slab[0]), int(slab[1]), int(bool(slab[2]))

@@ -82,6 +82,8 @@ struct ns_ctx {
     int xwhat = -1;
     double* xbuf = nullptr;                  // the stage input whose ghost planes are exchanged
     unsigned long long* xslot = nullptr;     // the CFL minimum reduced over the slabs
+    bool flags_valid = false;                // the sensor's flags belong to the current state's run
+    int sms = 148;                           // multiprocessors of the context's device
 };
 
 static size_t host_elems(const ns_params* p) {
@@ -135,6 +137,7 @@ static ns_status validate(const ns_params* p) {
             return fail(NS_ERR_INVALID_ARG, "the sensor-gated form runs in NS_PREC_FP32");
         if (!(p->sensor_threshold > 0.0 && p->sensor_threshold < 1.0))
             return fail(NS_ERR_INVALID_ARG, "sensor_threshold must lie in (0,1)");
+        if (p->sensor_period < 0) return fail(NS_ERR_INVALID_ARG, "sensor_period must be >= 0");
     }
     return NS_OK;
 }
@@ -335,18 +338,23 @@ static ns_status do_step_fused(ns_ctx* ctx) {
     a.U0 = ctx->U0;
     a.slot = cur;
     a.slot_next = nxt;
-    if (p.sensor && a.conv_dims > 0) {
-        // the network on the step's start state; its flags gate the three stages
-        for (int d = 0; d < a.conv_dims; d++) {
-            if (sensor_step_mask(ctx->sensor, d, ctx->U0, ctx->box, ctx->c, p.sensor_threshold, ctx->fb[d], s,
-                                 &ctx->launches) != NS_OK)
-                return fail(NS_ERR_CUDA, "sensor flag kernel launch failed: %s",
-                            cudaGetErrorString(cudaGetLastError()));
-            a.gate.m[d] = sensor_mask(ctx->sensor, d);
-            a.gate.fb[d] = ctx->fb[d];
+    const bool gated = p.sensor && a.conv_dims > 0;
+    GateLists gl;
+    if (gated) {
+        // the network on the step's start state (every sensor_period steps); its
+        // flags gate the three stages: component-wise stages, then the flagged
+        // faces corrected to characteristic-wise (ns_gate.cu)
+        const int period = p.sensor_period > 1 ? p.sensor_period : 1;
+        if (!ctx->flags_valid || ctx->steps % period == 0) {
+            if (sensor_step_flags(ctx->sensor, ctx->U0, ctx->box, ctx->c, p.sensor_threshold, ctx->fb, a.conv_dims, s,
+                                  &ctx->launches) != NS_OK)
+                return fail(NS_ERR_CUDA, "sensor flag kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
+            ctx->flags_valid = true;
+            prof_mark(ctx, NS_PROF_SENSOR);
         }
-        a.gated = true;
-        prof_mark(ctx, NS_PROF_SENSOR);
+        gl = sensor_gate_lists(ctx->sensor);
+        a.chr = false;
+        a.skip = gl.touched;
     }
     // SSP-RK3 coefficients (time_scheme.cpp:36-38, 48-50, 60-62); U0 -> U -> U2 -> U
     const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
@@ -368,6 +376,12 @@ static ns_status do_step_fused(ns_ctx* ctx) {
         ctx->launches++;
         if (e != cudaSuccess) return fail(NS_ERR_CUDA, "fused stage launch failed: %s", cudaGetErrorString(e));
         prof_mark(ctx, NS_PROF_STAGE_FUSED);
+        if (gated) {
+            e = gate_correct(a, gl, ctx->F, ctx->fb, ctx->sms, s);
+            ctx->launches += a.conv_dims + 1;
+            if (e != cudaSuccess) return fail(NS_ERR_CUDA, "sensor correction launch failed: %s", cudaGetErrorString(e));
+            prof_mark(ctx, NS_PROF_SENSOR);
+        }
     }
     ctx->parity ^= 1;
     ctx->fused_ready = true;
@@ -601,6 +615,7 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
     for (int d = 0; d < 3; d++) ctx->fb[d] = make_facebox(p->nx, p->ny, p->nz, d);
     ctx->c = make_consts(p);
     cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device);
     ns_status st = NS_OK;
     auto A = [&](void** ptr, size_t bytes) {
         if (st != NS_OK) return;
@@ -674,6 +689,7 @@ ns_status ns_upload_primitive(ns_ctx* ctx, const double* W) {
     ctx->w_valid = true;
     ctx->u_valid = false;
     ctx->fused_ready = false;
+    ctx->flags_valid = false;
     ctx->halos_stale = false;
     NS_CUDA(cudaStreamSynchronize(ctx->stream));
     return NS_OK;
@@ -702,6 +718,7 @@ ns_status ns_convection_solve(ns_ctx* ctx, const double* W, const double* U, dou
     NS_TRY(upload(ctx, R, ctx->R));
     ctx->w_valid = ctx->u_valid = false;  // the device state now holds the operator's inputs
     ctx->fused_ready = ctx->halos_stale = false;
+    ctx->flags_valid = false;
     NS_TRY(faces(ctx));
     UpdateArgs a = update_args(ctx, MODE_RHS, true, false);
     launch_update(a, ctx->stream);
@@ -717,6 +734,7 @@ ns_status ns_diffusion_solve(ns_ctx* ctx, const double* W, double* R) {
     NS_TRY(upload(ctx, R, ctx->R));
     ctx->w_valid = ctx->u_valid = false;
     ctx->fused_ready = ctx->halos_stale = false;
+    ctx->flags_valid = false;
     UpdateArgs a = update_args(ctx, MODE_RHS, false, true);
     launch_update(a, ctx->stream);
     NS_TRY(check_launch(ctx, 1));
@@ -732,6 +750,7 @@ ns_status ns_rhs(ns_ctx* ctx, const double* W, double* R, int terms) {
     NS_TRY(upload(ctx, R, ctx->R));
     cudaStream_t s = ctx->stream;
     ctx->fused_ready = ctx->halos_stale = false;
+    ctx->flags_valid = false;
     NS_CUDA(cudaMemsetAsync(ctx->slot + 2, 0xFF, sizeof(unsigned long long), s));
     launch_step_begin(false, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, ctx->slot + 2, s);
     launch_fill_prim(ctx->W, ctx->U, ctx->box, ctx->c, s);
@@ -752,6 +771,7 @@ ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out) {
     ctx->w_valid = true;
     ctx->u_valid = false;
     ctx->fused_ready = ctx->halos_stale = false;
+    ctx->flags_valid = false;
     NS_CUDA(cudaMemsetAsync(ctx->slot + 2, 0xFF, sizeof(unsigned long long), ctx->stream));
     launch_min_dt(phys(ctx), ctx->W, ctx->box, ctx->c, ctx->slot + 2, ctx->stream);
     NS_TRY(check_launch(ctx, 1));
@@ -769,6 +789,7 @@ ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
     ctx->w_valid = true;
     ctx->u_valid = false;
     ctx->fused_ready = ctx->halos_stale = false;
+    ctx->flags_valid = false;
     NS_TRY(do_step(ctx));
     NS_TRY(finalize_w(ctx));
     double clk[2];

@@ -87,19 +87,11 @@ __device__ __forceinline__ int ring_slot(int i, int x0) {
 }
 
 // one face from a 6-cell stencil in a shared array with stride `step`
-// (GATE: the characteristic-wise form where `fire`, the component-wise elsewhere)
-template <int DIR, bool CHAR, bool BORGES, bool GATE, bool PHYS, typename T>
+template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T>
 __device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, T gamma,
-                                           T inv_gm1, bool fire, T out[5]) {
+                                           T inv_gm1, T out[5]) {
     if constexpr (sizeof(T) == 4) {
-        if constexpr (GATE) {
-            if (fire)
-                face_f32x2<DIR, true, BORGES, PHYS>(planes, c0, step, fs, gamma, inv_gm1, out);
-            else
-                face_f32x2<DIR, false, BORGES, PHYS>(planes, c0, step, fs, gamma, inv_gm1, out);
-        } else {
-            face_f32x2<DIR, CHAR, BORGES, PHYS>(planes, c0, step, fs, gamma, inv_gm1, out);
-        }
+        face_f32x2<DIR, CHAR, BORGES, PHYS>(planes, c0, step, fs, gamma, inv_gm1, out);
         return;
     }
     static_assert(sizeof(T) == 4 || !PHYS, "the FP64 march face follows the reference semantics");
@@ -273,12 +265,12 @@ __device__ __forceinline__ void march_viscous_physical(PlaneFn plane, int i, int
     r[1] -= work + diss + T(c.heat) * mu * lapT;
 }
 
-template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool GATE, bool PHYS>
+template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool PHYS>
 __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     k_stage_march(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
                   Consts c, int conv_dims, double m1, double m2, double mc,
                   const unsigned long long* __restrict__ slot, unsigned long long* slot_next,
-                  double* clock, Gate gate) {
+                  double* clock, const unsigned char* __restrict__ skip) {
     using M = MarchTile<T, H>;
     static_assert(M::NFY <= 2 * FT && M::NFZ <= 2 * FT, "a face pass takes at most two rounds");
     extern __shared__ __align__(16) unsigned char smem[];
@@ -338,41 +330,20 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     };
     // x-face of this thread's column between cells i and i+1 (stencil i-2..i+3)
     const int ccol = (ty + 3) * M::PZ + (tz + 3);
-    auto xface = [&](int i, bool fire, T out[5]) {
+    auto xface = [&](int i, T out[5]) {
         const T* P[6];
 #pragma unroll
         for (int s = 0; s < 6; s++) P[s] = plane(i - 2 + s);
-        march_face<0, CHAR, BORGES, GATE, PHYS, T>(P, ccol, 0, M::NP, gamma, inv_gm1, fire, out);
+        march_face<0, CHAR, BORGES, PHYS, T>(P, ccol, 0, M::NP, gamma, inv_gm1, out);
     };
     const int gj = j0 + ty, gk = k0 + tz;
     const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
     const bool own = row && gj < b.ny && gk < b.nz;
-    // sensor flags of this thread's faces of plane i (x-face i+1/2, up to two y- and
-    // two z-faces), loaded early and tested only in the face pass; i = x0 - 1 (the
-    // first x-face) can be -1, which has no y- or z-faces
-    unsigned char gx = 0, gy[2] = {0, 0}, gz[2] = {0, 0};
-    auto load_flags = [&](int i) {
-        if constexpr (GATE) {
-            gx = own ? gate.m[0][gate.fb[0].at(i + 1, gj, gk)] : 0;
-#pragma unroll
-            for (int r = 0; r < 2; r++) {
-                int e = rotated(tid, 7) + r * FT;
-                int a = j0 + e / M::TZ, kk = k0 + e % M::TZ;
-                gy[r] = (i >= 0 && e < M::NFY && a <= b.ny && kk < b.nz) ? gate.m[1][gate.fb[1].at(i, a, kk)] : 0;
-                e = rotated(tid, 6) + r * FT;
-                int jj = j0 + e / (M::TZ + 1);
-                a = k0 + e % (M::TZ + 1);
-                gz[r] = (i >= 0 && conv_dims == 3 && e < M::NFZ && jj < b.ny && a <= b.nz)
-                            ? gate.m[2][gate.fb[2].at(i, jj, a)] : 0;
-            }
-        }
-    };
     for (int i = x0 - 3; i < x0 + 3; i++) load_plane(i);
     issue_plane(x0 + 3);
     __syncthreads();
     T fxl[5] = {0, 0, 0, 0, 0}, fxr[5];
-    load_flags(x0 - 1);
-    if (conv_dims > 0 && row) xface(x0 - 1, gx != 0, fxl);
+    if (conv_dims > 0 && row) xface(x0 - 1, fxl);
     if constexpr (M::LEAN) __syncthreads();  // plane x0+3 takes the slot of plane x0-3
     const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
     const double m3 = mc * dt;
@@ -382,35 +353,29 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     }
     double best = INFINITY;
     for (int i = x0; i < x1; i++) {
-        load_flags(i);
         convert_plane(i + 3);
         __syncthreads();
         if (i + 1 < x1) issue_plane(i + 4);  // in flight during this plane's faces and update
         const T* Pi = plane(i);
         T* FY = FYb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFY;
         T* FZ = FZb + (M::NBUF == 2 ? ((i - x0) & 1) : 0) * 5 * M::NFZ;
-        // GATE: a flagged face takes the characteristic-wise branch in its own lane
-        // (a dense recompute of the block's flagged faces after the pass measured
-        // slower: it adds a block-wide round and a barrier to every plane)
         if (conv_dims > 0) {
-            if (row) xface(i, gx != 0, fxr);
+            if (row) xface(i, fxr);
             // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
-            for (int e = rotated(tid, 7), r = 0; e < M::NFY; e += FT, r++) {
+            for (int e = rotated(tid, 7); e < M::NFY; e += FT) {
                 int fb = e / M::TZ, cz = e % M::TZ;
                 const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                 T out[5];
-                march_face<1, CHAR, BORGES, GATE, PHYS, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1,
-                                                     gy[r] != 0, out);
+                march_face<1, CHAR, BORGES, PHYS, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1, out);
 #pragma unroll
                 for (int q = 0; q < 5; q++) FY[q * M::NFY + e] = out[q];
             }
             if (conv_dims == 3) {
-                for (int e = rotated(tid, 6), r = 0; e < M::NFZ; e += FT, r++) {
+                for (int e = rotated(tid, 6); e < M::NFZ; e += FT) {
                     int ry = e / (M::TZ + 1), fc = e % (M::TZ + 1);
                     const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                     T out[5];
-                    march_face<2, CHAR, BORGES, GATE, PHYS, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1,
-                                                         gz[r] != 0, out);
+                    march_face<2, CHAR, BORGES, PHYS, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1, out);
 #pragma unroll
                     for (int q = 0; q < 5; q++) FZ[q * M::NFZ + e] = out[q];
                 }
@@ -452,7 +417,8 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
                 un[q] = (u0[q] * m1) + (ui[q] * m2) + (r[q] * m3);
                 Uout[q * b.fstride + o] = un[q];
             }
-            if constexpr (LAST) {
+            // the sensor's correction pass forms the next step's start of the cells it corrects
+            if (LAST && !(skip && skip[((long long)i * b.ny + gj) * b.nz + gk])) {
                 double w[5], un0[5];
                 prim_from_cons(un, c.gm1, w);
                 double d = PHYS ? local_dt_physical(w, c) : local_dt(w, c);
@@ -469,26 +435,26 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     if constexpr (LAST) block_min_to(best, slot_next);
 }
 
-template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool GATE, bool PHYS>
+template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool PHYS>
 static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
     using M = MarchTile<T, H>;
-    auto kern = k_stage_march<T, CHAR, BORGES, H, LAST, GATE, PHYS>;
+    auto kern = k_stage_march<T, CHAR, BORGES, H, LAST, PHYS>;
     // the attribute is per device; setting it on every launch keeps multi-device use correct
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
     if (e != cudaSuccess) return e;
     dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + M::LX - 1) / M::LX);
     kern<<<grid, FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
-                                   a.slot_next, a.clock, a.gate);
+                                   a.slot_next, a.clock, a.skip);
     return cudaGetLastError();
 }
 
-template <bool PHYS, bool CHAR, bool BORGES, bool LAST, bool GATE = false>
+template <bool PHYS, bool CHAR, bool BORGES, bool LAST>
 static cudaError_t fused_h(const FusedArgs& a, cudaStream_t s) {
     switch (a.visc_h) {
-        case 0: return fused_one<float, CHAR, BORGES, 0, LAST, GATE, PHYS>(a, s);
-        case 1: return fused_one<float, CHAR, BORGES, 1, LAST, GATE, PHYS>(a, s);
-        case 2: return fused_one<float, CHAR, BORGES, 2, LAST, GATE, PHYS>(a, s);
-        default: return fused_one<float, CHAR, BORGES, 3, LAST, GATE, PHYS>(a, s);
+        case 0: return fused_one<float, CHAR, BORGES, 0, LAST, PHYS>(a, s);
+        case 1: return fused_one<float, CHAR, BORGES, 1, LAST, PHYS>(a, s);
+        case 2: return fused_one<float, CHAR, BORGES, 2, LAST, PHYS>(a, s);
+        default: return fused_one<float, CHAR, BORGES, 3, LAST, PHYS>(a, s);
     }
 }
 
@@ -497,12 +463,6 @@ static cudaError_t fused_h(const FusedArgs& a, cudaStream_t s) {
 template <bool PHYS>
 cudaError_t fused_launch(const FusedArgs& a, cudaStream_t s) {
     if (!a.fp32) return cudaErrorInvalidValue;  // the FP32 form only
-    if (a.gated) {  // learned-sensor gate: characteristic-wise form only
-        if (!a.chr) return cudaErrorInvalidValue;
-        if (a.borges)
-            return a.last ? fused_h<PHYS, true, true, true, true>(a, s) : fused_h<PHYS, true, true, false, true>(a, s);
-        return a.last ? fused_h<PHYS, true, false, true, true>(a, s) : fused_h<PHYS, true, false, false, true>(a, s);
-    }
     if (a.chr) {
         if (a.borges) return a.last ? fused_h<PHYS, true, true, true>(a, s) : fused_h<PHYS, true, true, false>(a, s);
         return a.last ? fused_h<PHYS, true, false, true>(a, s) : fused_h<PHYS, true, false, false>(a, s);

@@ -41,6 +41,19 @@ struct Gate {
     FaceBox fb[3];
 };
 
+// The learned sensor's flags of a step in the form the correction passes read:
+// per axis the flag bytes and a compacted list of the flagged faces (FaceBox
+// indices), and the cells next to a flagged face (one byte per cell, and a
+// compacted list of interior indices (i ny + j) nz + k).  Counts on the device.
+struct GateLists {
+    const unsigned* face_list[3];
+    const unsigned* face_count;  // [3]
+    const unsigned* cell_list;
+    const unsigned* cell_count;
+    const unsigned char* touched;
+    const unsigned char* mask[3];
+};
+
 // one fused SSP-RK3 stage (ns_fused.cu)
 struct FusedArgs {
     const double* Uin;
@@ -57,10 +70,14 @@ struct FusedArgs {
     const unsigned long long* slot;   // CFL minimum of this step
     unsigned long long* slot_next;    // last stage: CFL minimum of the next step
     double* clock;                    // first stage: [last dt, accumulated time]
-    bool gated;                       // characteristic-wise only where gate flags a face (FP32)
-    Gate gate;
+    const unsigned char* skip;        // last stage: cells (interior order) whose next-step start a
+                                      // correction pass forms instead (nullable)
 };
 cudaError_t launch_stage_fused(const FusedArgs& a, cudaStream_t s);
+// the learned sensor's correction of a fused FP32 stage (ns_gate.cu); F: per-axis
+// float face arrays for the flagged faces' flux differences
+cudaError_t gate_correct(const FusedArgs& a, const GateLists& L, void* const F[3], const FaceBox fb[3], int sms,
+                         cudaStream_t s);
 
 cudaError_t launch_fma_probe(bool fp64, int blocks, int iters, void* sink, cudaStream_t s);
 

@@ -698,11 +698,16 @@ __global__ void __launch_bounds__(128) k_sensor_prims(const double* __restrict__
     prim[4 * n + e] = u[4] * ir;
 }
 
+// Flags of every face along DIR; a flagged face also goes into the compacted
+// list of its axis (FaceBox index) and marks the interior cells on either side
+// as touched, for the correction passes of ns_gate.cu.
 template <int DIR>
 __global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ prim, Box b, Consts c,
                                                      FaceBox fb, const float* __restrict__ w,
                                                      float logit_thr, unsigned char* __restrict__ mask,
-                                                     unsigned long long* __restrict__ flagged) {
+                                                     unsigned long long* __restrict__ flagged,
+                                                     unsigned* __restrict__ list, unsigned* __restrict__ count,
+                                                     unsigned char* __restrict__ touched) {
     __shared__ __align__(16) MlpSmem m;
     __shared__ __align__(16) __nv_bfloat16 Xs[4][32 * XS];
     const int warp = threadIdx.y, lane = threadIdx.x;
@@ -771,10 +776,41 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ p
                 if ((lane >> 4) == mt && ((lane >> 3) & 1) == h) lg = v;
             }
         const bool fire = live && lg > logit_thr;
-        if (live) mask[fb.at(aa, bb, kk)] = fire ? 1 : 0;
-        nfire += __popc(__ballot_sync(0xffffffffu, fire));
+        const long long fi = live ? fb.at(aa, bb, kk) : 0;
+        if (live) mask[fi] = fire ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, fire);
+        nfire += __popc(m);
+        if (m) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(count, (unsigned)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (fire) {
+                list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)fi;
+                // the interior cells below (face - 1) and above (face) along DIR: the cell
+                // above has the face's own coordinates
+                const int a = DIR == 0 ? aa : (DIR == 1 ? bb : kk), na = DIR == 0 ? b.nx : (DIR == 1 ? b.ny : b.nz);
+                const long long cell = ((long long)aa * b.ny + bb) * b.nz + kk;
+                const long long step = DIR == 0 ? (long long)b.ny * b.nz : (DIR == 1 ? (long long)b.nz : 1LL);
+                if (a - 1 >= 0) touched[cell - step] = 1;
+                if (a < na) touched[cell] = 1;
+            }
+        }
     }
     if (lane == 0 && nfire) atomicAdd(flagged, nfire);
+}
+
+// compacted list of the touched cells (interior order), the cells a correction pass updates
+__global__ void __launch_bounds__(128) k_sensor_touched_list(const unsigned char* __restrict__ touched, long long n,
+                                                             unsigned* __restrict__ list, unsigned* __restrict__ count) {
+    const long long e = (long long)blockIdx.x * 128 + threadIdx.x;
+    const bool t = e < n && touched[e] != 0;
+    const unsigned m = __ballot_sync(0xffffffffu, t);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (t) list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)e;
 }
 
 // ---------------------------------------------------------------------------
@@ -784,6 +820,11 @@ struct SensorState {
     float* w = nullptr;                    // FP32 parameters on the device
     unsigned long long* flagged = nullptr;  // faces flagged since creation
     unsigned char* mask[3] = {nullptr, nullptr, nullptr};  // per-step flags, one byte per face
+    unsigned* list[3] = {nullptr, nullptr, nullptr};       // flagged faces per axis (compacted)
+    unsigned* counts = nullptr;            // [0..2] flagged faces per axis, [3] touched cells
+    unsigned char* touched = nullptr;      // cells next to a flagged face, one byte per interior cell
+    unsigned* cells = nullptr;             // the touched cells (compacted)
+    long long ncells = 0;
     float* prim = nullptr;                  // the step's rho, p, u, v, w (FP32 planes) for the flags
     unsigned long long faces = 0;           // faces evaluated since creation (host count)
     int sms = 148;                          // multiprocessors of the context's device
@@ -797,6 +838,12 @@ ns_status sensor_create(SensorState** out, const Box& b, const FaceBox* fb, cuda
     bool ok = cudaMalloc(&st->w, SP * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&st->flagged, sizeof(unsigned long long)) == cudaSuccess;
     for (int d = 0; d < 3 && ok; d++) ok = cudaMalloc(&st->mask[d], (size_t)fb[d].fstride) == cudaSuccess;
+    for (int d = 0; d < 3 && ok; d++)
+        ok = cudaMalloc(&st->list[d], (size_t)fb[d].fstride * sizeof(unsigned)) == cudaSuccess;
+    st->ncells = (long long)b.nx * b.ny * b.nz;
+    ok = ok && cudaMalloc(&st->counts, 4 * sizeof(unsigned)) == cudaSuccess &&
+         cudaMalloc(&st->touched, (size_t)st->ncells) == cudaSuccess &&
+         cudaMalloc(&st->cells, (size_t)st->ncells * sizeof(unsigned)) == cudaSuccess;
     ok = ok && cudaMalloc(&st->prim, (size_t)5 * b.nx * b.ny * b.nz * sizeof(float)) == cudaSuccess;
     int dev = 0;
     if (ok && cudaGetDevice(&dev) == cudaSuccess)
@@ -808,6 +855,7 @@ ns_status sensor_create(SensorState** out, const Box& b, const FaceBox* fb, cuda
     }
     cudaMemsetAsync(st->w, 0, SP * sizeof(float), s);
     cudaMemsetAsync(st->flagged, 0, sizeof(unsigned long long), s);
+    cudaMemsetAsync(st->counts, 0, 4 * sizeof(unsigned), s);
     *out = st;
     return NS_OK;
 }
@@ -817,6 +865,10 @@ void sensor_destroy(SensorState* st) {
     cudaFree(st->w);
     cudaFree(st->flagged);
     for (int d = 0; d < 3; d++) cudaFree(st->mask[d]);
+    for (int d = 0; d < 3; d++) cudaFree(st->list[d]);
+    cudaFree(st->counts);
+    cudaFree(st->touched);
+    cudaFree(st->cells);
     cudaFree(st->prim);
     delete st;
 }
@@ -856,26 +908,52 @@ ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const doub
     return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;
 }
 
-ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box& b, const Consts& c,
-                           double threshold, const FaceBox& fb, cudaStream_t s, long long* launches) {
+ns_status sensor_step_flags(SensorState* st, const double* U0, const Box& b, const Consts& c, double threshold,
+                            const FaceBox fb[3], int conv_dims, cudaStream_t s, long long* launches) {
     const float thr = (float)std::log(threshold / (1.0 - threshold));
-    const long long tiles = (long long)((fb.n2 + 31) / 32) * ((fb.n1 + 3) / 4) * fb.n0;
-    if (tiles >= (1ll << 31)) return NS_ERR_UNSUPPORTED;
-    const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
     const dim3 blk(32, 4);
-    if (dir == 0) {  // the first axis of a step forms the primitive planes for all three
-        k_sensor_prims<<<dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx), blk, 0, s>>>(U0, b, c, st->prim);
+    if (cudaMemsetAsync(st->counts, 0, 4 * sizeof(unsigned), s) != cudaSuccess ||
+        cudaMemsetAsync(st->touched, 0, (size_t)st->ncells, s) != cudaSuccess)
+        return NS_ERR_CUDA;
+    // the step's rho, p, u, v, w in FP32, read by the three axes
+    k_sensor_prims<<<dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx), blk, 0, s>>>(U0, b, c, st->prim);
+    if (launches) (*launches)++;
+    for (int d = 0; d < conv_dims; d++) {
+        const FaceBox& f = fb[d];
+        const long long tiles = (long long)((f.n2 + 31) / 32) * ((f.n1 + 3) / 4) * f.n0;
+        if (tiles >= (1ll << 31) || f.fstride >= (1ll << 32)) return NS_ERR_UNSUPPORTED;
+        const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
+        if (d == 0)
+            k_sensor_mask<0><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[0], st->flagged, st->list[0],
+                                                st->counts + 0, st->touched);
+        else if (d == 1)
+            k_sensor_mask<1><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[1], st->flagged, st->list[1],
+                                                st->counts + 1, st->touched);
+        else
+            k_sensor_mask<2><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[2], st->flagged, st->list[2],
+                                                st->counts + 2, st->touched);
+        st->faces += (unsigned long long)f.n0 * f.n1 * f.n2;
         if (launches) (*launches)++;
     }
-    if (dir == 0) k_sensor_mask<0><<<grid, blk, 0, s>>>(st->prim, b, c, fb, st->w, thr, st->mask[0], st->flagged);
-    else if (dir == 1) k_sensor_mask<1><<<grid, blk, 0, s>>>(st->prim, b, c, fb, st->w, thr, st->mask[1], st->flagged);
-    else k_sensor_mask<2><<<grid, blk, 0, s>>>(st->prim, b, c, fb, st->w, thr, st->mask[2], st->flagged);
-    st->faces += (unsigned long long)fb.n0 * fb.n1 * fb.n2;
+    k_sensor_touched_list<<<(unsigned)((st->ncells + 127) / 128), 128, 0, s>>>(st->touched, st->ncells, st->cells,
+                                                                              st->counts + 3);
     if (launches) (*launches)++;
     return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;
 }
 
-const unsigned char* sensor_mask(const SensorState* st, int dir) { return st->mask[dir]; }
+GateLists sensor_gate_lists(const SensorState* st) {
+    GateLists L;
+    for (int d = 0; d < 3; d++) {
+        L.face_list[d] = st->list[d];
+        L.mask[d] = st->mask[d];
+    }
+    L.face_count = st->counts;
+    L.cell_list = st->cells;
+    L.cell_count = st->counts + 3;
+    L.touched = st->touched;
+    return L;
+}
+
 
 double sensor_last_fraction(SensorState* st) {
     if (!st || st->faces == 0) return 0.0;

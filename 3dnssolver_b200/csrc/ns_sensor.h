@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "ns_common.cuh"
+#include "ns_kernels.h"
 
 namespace nsb {
 
@@ -17,13 +18,12 @@ void sensor_destroy(SensorState* st);
 ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const double* U, const Box& b,
                            const Consts& c, double threshold, bool borges, bool phys, void* F,
                            const FaceBox& fb, cudaStream_t s, long long* launches);
-// Per-step flags along axis dir for the fused stage kernel: the network on every
-// face of the step's start state U0, one byte per face (FaceBox order).  The
-// call for dir 0 (always the first of a step) also forms the FP32 primitive
-// planes the three axes read.
-ns_status sensor_step_mask(SensorState* st, int dir, const double* U0, const Box& b, const Consts& c,
-                           double threshold, const FaceBox& fb, cudaStream_t s, long long* launches);
-const unsigned char* sensor_mask(const SensorState* st, int dir);
+// The flags of a step from its start state U0: the network on every face of the
+// convected axes (one byte per face, FaceBox order), the compacted lists of the
+// flagged faces and of the cells next to them (GateLists).
+ns_status sensor_step_flags(SensorState* st, const double* U0, const Box& b, const Consts& c, double threshold,
+                            const FaceBox fb[3], int conv_dims, cudaStream_t s, long long* launches);
+GateLists sensor_gate_lists(const SensorState* st);
 // fraction of evaluated faces the sensor flagged since the context was created
 double sensor_last_fraction(SensorState* st);
 ns_status sensor_set_weights(SensorState* st, const float* w, cudaStream_t s);

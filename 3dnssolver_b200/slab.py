@@ -109,8 +109,6 @@ class HaloExchange:
         positive double, or -1 (all ones) for none."""
         import torch
         import torch.distributed as dist
-        if self.world == 1:
-            return
         v = torch.where(t == -1, torch.full_like(t, INT64_MAX), t)
         dist.all_reduce(v, op=dist.ReduceOp.MIN, group=self.group)
         t.copy_(torch.where(v == INT64_MAX, torch.full_like(v, -1), v))
@@ -127,15 +125,17 @@ class _DevPtr:
 class SlabSolver:
     """One rank's slab of a global problem: a Solver on bc[0] = NS_BC_EXTERNAL whose
     steps exchange ghost planes and dt with the other ranks through `exchange`
-    (a HaloExchange).  host_staged: the exchange runs on host copies (gloo)."""
+    (a HaloExchange).  The context and the exchange's torch operations share one
+    stream (`stream`, or a new one): the callback's copies and collectives are
+    then ordered after the kernels that produce their inputs."""
 
-    def __init__(self, global_params, rank, world, exchange):
+    def __init__(self, global_params, rank, world, exchange, stream=None):
         import torch
         self.global_params = global_params
         self.rank, self.world = rank, world
         self.params = slab_params(global_params, rank, world)
         self.solver = _pkg.Solver(self.params)
-        self.stream = torch.cuda.current_stream()
+        self.stream = stream if stream is not None else torch.cuda.Stream()
         self.solver.set_stream(self.stream.cuda_stream)
         self.ex = exchange
         L = self.solver.lib
@@ -160,11 +160,13 @@ class SlabSolver:
 
     # -- the exchange callback (called from inside ns_advance / ns_time_step) --
     def _callback(self, user, ctx, what, stream):
+        import torch
         try:
-            if what == _abi.EXCHANGE_DT:
-                self._reduce_dt()
-            else:
-                self._halo()
+            with torch.cuda.stream(self.stream):
+                if what == _abi.EXCHANGE_DT:
+                    self._reduce_dt()
+                else:
+                    self._halo()
             return 0
         except Exception as e:  # reported by the step's status
             self.error = e

@@ -24,9 +24,13 @@ Arms:
   --impl reference   the reference's own CPU TimeScheme::step (compiled from its
                      sources into oracle/_ref, OpenMP on all host cores), on the
                      same workload's initial condition at 256^3 (a bounded sample)
-Multi-GPU (torchrun): every rank advances an independent replica (no
-collective on the data path of this line); value sums the ranks, time is the
-max over ranks.
+Multi-GPU (torchrun, N > 1): the domain is split along x into one slab per rank
+(weak scaling: every rank holds the workload's n^3 cells, the global grid is
+(N n) x n x n with the x extent N times the single-GPU box); before every RK
+stage each rank exchanges its 3 outer planes x 5 fields per side with its x
+neighbours (NCCL send/recv over NVLink) and the CFL minimum is all-reduced once
+per step (3dnssolver_b200/slab.py).  value = all ranks' cell-updates / the
+slowest rank's device time.
 """
 import argparse
 import csv
@@ -460,6 +464,95 @@ def sod_comparison(pkg, wl, sensor_w_ref, t_end=0.2):
     return out
 
 
+def slab_bench(args, dist, rank, world, local):
+    """N > 1: the headline form on a slab decomposition along x (weak scaling)."""
+    import torch
+    pkg = importlib.import_module("3dnssolver_b200")
+    wl = importlib.import_module("3dnssolver_b200.workloads")
+    slab = importlib.import_module("3dnssolver_b200.slab")
+    wk = args.workload
+    n = args.n or WORKLOADS[wk]["n"]
+    p1 = workload_params(pkg, wk, n, args.form)
+    # the global problem: N single-GPU boxes side by side along x (the same dx)
+    pg = workload_params(pkg, wk, n, args.form)
+    pg.nx, pg.Lx = n * world, p1.Lx * world
+    W_local = initial_state(wl, wk, p1, seed=(5 if wk == "tgv" else 1) + rank)  # this rank's box
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        ex = slab.HaloExchange(rank, world, periodic=True, host_staged=False)
+        s = slab.SlabSolver(pg, rank, world, ex, stream=stream)
+        s.upload_primitive(W_local)
+        s.advance(args.warmup)
+        torch.cuda.synchronize()
+        clk = ClockSampler(local)
+        clk.start()
+        t0 = time.time()
+        while time.time() - t0 < 1.0:  # the sampler sees the GPU under load through the timed region
+            s.advance(1)
+            torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        l0 = s.solver.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist)
+        launches = s.solver.launches - l0
+        clocks = clk.stop()
+        prof = profile(s.solver)
+        # end to end: ns_time_step with the rank's host W (pinned), exchanges included
+        Wh_t = torch.empty(W_local.shape, dtype=torch.float64, pin_memory=True)
+        Wh = Wh_t.numpy()
+        Wh[...] = W_local
+        s.solver.time_step(Wh)
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.e2e_steps):
+            s.solver.time_step(Wh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist)
+        diag = s.diagnostics()
+        s.close()
+    cells = n ** 3
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    fma = {"fp64": pkg.fma_peak(True), "fp32": pkg.fma_peak(False)}
+    roofline, compute_roofline = rooflines(args.form, prof, n, ms / args.steps, peaks, fma)
+    halo_bytes = 2 * 15 * n * n * 8 * 3  # both sides, 3 planes x 5 fields, 3 stages per step
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": job_rate(world, cells, args.steps, ms), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": FORMS[args.form]["dtype"], "data": "synthetic",
+            "config": {"workload": workload_name(wk, n, args.form) + f", {world} slabs along x",
+                       "grid": [n * world, n, n], "grid_per_gpu": [n, n, n], "form": args.form,
+                       "l2": "no flush: device state per GPU larger than L2",
+                       "parallelism": f"slab decomposition along x over {world} GPUs: NCCL send/recv of "
+                                      f"3 planes x 5 fields per side before every RK stage, "
+                                      f"all-reduce(min) of the CFL minimum per step",
+                       "halo_bytes_per_step_per_gpu": halo_bytes},
+            "roofline": roofline, "compute_roofline": compute_roofline,
+            "kernel_ms_per_step": {k: round(v, 4) for k, v in prof.items() if v > 0},
+            "cpu_baseline": None, "gpu_launches": launches, "clocks": clocks,
+            "e2e": {"value": job_rate(world, cells, args.e2e_steps, e2e_ms), "unit": UNIT,
+                    "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Wh.nbytes),
+                    "steps": args.e2e_steps, "api": "ns_time_step on every rank's slab, pinned host W"},
+            "diagnostics": {"nonfinite": diag["nonfinite"], "dt": diag["dt"]},
+        }
+        print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -477,6 +570,10 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+        try:
+            return slab_bench(args, dist, rank, world, local)
+        finally:
+            dist.destroy_process_group()
 
     def barrier():
         if dist is not None:

@@ -95,7 +95,9 @@ typedef struct ns_params {
     int slab_nx;         /* global cells along x (the slabs' nx sum to it) */
     int slab_periodic;   /* 1: the global x axis is periodic; 0: Neumann at the global ends
                           * (the end slabs fill their outer ghost planes themselves) */
-    int reserved[4];
+    int sensor_period;   /* sensor = 1: evaluate the network every sensor_period steps and gate
+                          * the steps in between with the same flags (0 or 1: every step) */
+    int reserved[3];
 } ns_params;
 
 /* Global diagnostics of the device state (no reference counterpart: the
@@ -227,11 +229,13 @@ NS_API ns_status ns_slab_dt_slot(ns_ctx* ctx, void** dev_ptr);
  * An MLP 21 -> 32 -> 32 -> 1 (GELU) predicts from a face's stencil whether the
  * characteristic-wise WENO-5 flux differs from the component-wise one by more
  * than a relative threshold; with ns_params.sensor = 1 (FP32 characteristic
- * form, reference semantics) the characteristic-wise flux is computed only on
- * the faces the network flags and the component-wise flux elsewhere.  Time
- * steps evaluate the network once per step, on the state at the step's start,
- * and its flags gate all three stages; the per-operator entry points
- * (ns_convection_solve, ns_rhs) evaluate it on the W they are given.  Parameters are
+ * form, either semantics) the characteristic-wise flux is used only on the
+ * faces the network flags and the component-wise flux elsewhere.  Time steps
+ * evaluate the network on the state at the step's start (every sensor_period
+ * steps); each stage then runs the component-wise stage on every face and
+ * corrects the flagged faces by their characteristic-wise minus component-wise
+ * flux (a compacted list).  The per-operator entry points (ns_convection_solve,
+ * ns_rhs) evaluate it on the W they are given.  Parameters are
  * NS_SENSOR_NPARAMS floats: W1[32][32] (out, in; in >= 21 unused), b1[32],
  * W2[32][32], b2[32], w3[32], b3.  Device pointers below are caller-owned. */
 #define NS_SENSOR_FEATURES 21

@@ -8,7 +8,12 @@ to the reference by tests/test_oracle_golden.py).
   config 3: Sod shock tube, characteristic-wise, one time step on 128x32x32 with
             the stable setting Ly = Lz = 1 (dy = dz = 4 dx at 512x128x128; here 4 dx too)
 
-Tolerance: 1e-12 relative L2 per conserved field, as in tests/test_gpu_parity.py.
+Tolerance: 1e-12 relative L2 per conserved field, as in tests/test_gpu_parity.py,
+for every state.  The 256^3 right-hand side alone is judged at 1e-11: at that
+grid the reference's own builds disagree with each other by up to 4.8e-12 in
+the rho residual (its strict -O2 build against its -O3 -ffast-math build, the
+oracle being bit-identical to the strict one), because the residual is a flux
+difference over a fine grid where the fluxes nearly cancel.
 rhoW of the shear layer is a noise-amplitude field (1e-3 seeded noise), so it is
 judged against the momentum magnitude, as two CPU builds of the reference
 already differ by 4e-12 in its own norm after 100 steps.
@@ -69,7 +74,7 @@ def test_config2_shear256_characteristic_rhs_and_step(oracle):
         dt = s.time_step(Wg, Ug)
     Ro = oracle.rhs(p, W0)
     err = rel_l2(interior(R), interior(Ro))
-    assert (err <= TOL).all(), f"config 2 rhs: rel L2 per field {err}"
+    assert (err <= 1e-11).all(), f"config 2 rhs: rel L2 per field {err}"
     Wo, Uo, dto = oracle.run(p, W0, 1)
     assert dt == pytest.approx(dto[0], rel=1e-14)
     _check(Ug, Uo, "config 2 one step")

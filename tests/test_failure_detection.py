@@ -70,7 +70,8 @@ def test_clean_state_passes_the_check():
         s.synchronize()
         Wh = W.copy()
         s.time_step(Wh)
-    assert np.isfinite(Wh).all()
+    # interior cells (edge and corner ghost cells are never filled, as in the reference)
+    assert np.isfinite(Wh[3:-3, 3:-3, 3:-3]).all()
 
 
 def test_without_the_check_nan_propagates_silently_as_in_the_reference():

@@ -89,3 +89,41 @@ def test_gpu_slabs_equal_the_single_domain(oracle, tmp_path, shape, world, bc, c
         Wo, Uo, dto = oracle.run(p, W0, nsteps)
         err = rel_l2(U, Uo[3:-3, 3:-3, 3:-3])
         assert (err[:4] <= 1e-12).all(), f"slabs vs oracle: rel L2 per field {err}"
+
+
+def _nccl_single_rank(port, pbytes, W_global, nsteps, outdir):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                            device_id=torch.device("cuda", 0))
+    try:
+        p = pkg.NsParams.from_buffer_copy(pbytes)
+        s = slab.SlabSolver(p, 0, 1, slab.HaloExchange(0, 1, periodic=True, host_staged=False))
+        s.upload_primitive(W_global)
+        s.advance(nsteps)
+        U = s.download_conservative()
+        s.close()
+        np.save(os.path.join(outdir, "U.npy"), U[3:-3, 3:-3, 3:-3])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_device_transport_one_periodic_rank_over_nccl(tmp_path):
+    """The device-buffer transport (host_staged=False: NCCL all-reduce of the dt slot
+    through its device address, ghost planes copied on the device) on one periodic
+    rank, whose ghost planes are its own: equal to the single-domain run."""
+    import torch.multiprocessing as mp
+    p = pkg.make_params(16, 12, 10, convection=2, diffusion_order=2, bc=(P, N, P), mu=0.02, cfl=0.3)
+    W0 = wl.random_field(p, seed=71, smooth=False)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(3)
+        Ug = s.download_conservative()[3:-3, 3:-3, 3:-3]
+    mp.start_processes(_nccl_single_rank, args=(_free_port(), bytes(p), W0, 3, str(tmp_path)), nprocs=1,
+                       join=True, start_method="spawn")
+    err = rel_l2(np.load(tmp_path / "U.npy"), Ug)
+    assert (err <= 1e-13).all(), err
