@@ -70,6 +70,9 @@ FORMS = {
     "fp32_comp": dict(conv=1, prec=1, dtype="f32 (f64 RK3 accumulation and reductions)"),
     "fp32_sensor": dict(conv=2, prec=1, sensor=1,
                         dtype="f32 + bf16 sensor (f64 RK3 accumulation and reductions)"),
+    # the network evaluated every 4th step, its flags gating the steps in between
+    "fp32_sensor_p4": dict(conv=2, prec=1, sensor=1, period=4,
+                           dtype="f32 + bf16 sensor (f64 RK3 accumulation and reductions)"),
     # the rest of the operator surface at full size: CD-6 viscous terms and Borges weights
     "fp64_char_cd6_borges": dict(conv=2, prec=0, order=6, weights=1, ref=None, dtype="f64"),
     "fp32_char_cd6_borges": dict(conv=2, prec=1, order=6, weights=1, ref="fp64_char_cd6_borges",
@@ -87,8 +90,8 @@ def parse():
     ap.add_argument("--workload", default="tgv", choices=sorted(WORKLOADS))
     ap.add_argument("--n", type=int, default=0, help="cells per axis (0: the workload's own)")
     ap.add_argument("--form", default="fp64_char", choices=sorted(FORMS))
-    ap.add_argument("--also", default="fp64_comp,fp32_char,fp32_comp,fp32_sensor,fp64_char_cd6_borges,"
-                                      "fp32_char_cd6_borges",
+    ap.add_argument("--also", default="fp64_comp,fp32_char,fp32_comp,fp32_sensor,fp32_sensor_p4,"
+                                      "fp64_char_cd6_borges,fp32_char_cd6_borges",
                     help="extra forms timed after the headline (comma list, '' for none)")
     ap.add_argument("--accuracy-steps", type=int, default=0,
                     help="steps of the per-form accuracy runs (0: warmup + steps)")
@@ -106,7 +109,8 @@ def workload_params(pkg, wk, n, form):
     return pkg.make_params(n, n, n, L=(L, L, L), mu=W["mu"], Pr=W["Pr"], gamma=1.4, cfl=W["cfl"],
                            convection=F["conv"], weights=F.get("weights", 0),
                            diffusion_order=F.get("order", 2), precision=F["prec"],
-                           semantics=W["semantics"], sensor=F.get("sensor", 0))
+                           semantics=W["semantics"], sensor=F.get("sensor", 0),
+                           sensor_period=F.get("period", 1))
 
 
 def workload_name(wk, n, form):
