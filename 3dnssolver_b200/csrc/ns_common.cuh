@@ -98,13 +98,6 @@ NS_HOST_DEVICE int fold(int i, int n, int periodic) {
     return i < 0 ? 0 : n - 1;
 }
 
-// x index of a stencil cell outside the interior along x: folded like fold() on
-// a single domain; on a slab the ghost planes hold the neighbours' cells (or the
-// Neumann copy at a global end), so the index is used as it is.
-NS_HOST_DEVICE int fold_x(int i, int nx, const Consts& c) {
-    return c.ext_x ? i : fold(i, nx, c.periodic[0]);
-}
-
 // Whether column i (interior coordinate) lies inside the global domain along x or
 // the global x axis is periodic: the reference's derivative ghost cells are zero
 // outside (centered_diffusion.cpp:22-24 fills them only by communication).
@@ -122,6 +115,18 @@ NS_HOST_DEVICE bool x_exchanged(int hi, int nx, const Consts& c) {
     if (!c.ext_x) return false;
     if (c.xper) return true;
     return hi ? (c.x0 + nx < c.nxg) : (c.x0 > 0);
+}
+
+// x index of a stencil cell outside the interior along x: folded like fold() on
+// a single domain; on a slab an exchanged side's ghost planes hold the
+// neighbour's cells, so the index is used as it is, and a side at a
+// non-periodic global end folds like Neumann (its ghost planes are copies of
+// the first interior plane).
+NS_HOST_DEVICE int fold_x(int i, int nx, const Consts& c) {
+    if (!c.ext_x) return fold(i, nx, c.periodic[0]);
+    if (i < 0 && !x_exchanged(0, nx, c)) return 0;
+    if (i >= nx && !x_exchanged(1, nx, c)) return nx - 1;
+    return i;
 }
 
 // ---------------------------------------------------------------------------

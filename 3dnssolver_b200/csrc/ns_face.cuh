@@ -142,13 +142,13 @@ __device__ __forceinline__ void half_flux(const T w[5], T hg, T f[5]) {
     f[4] = hrq * w[4] + (DIR == 2 ? half * p : T(0));
 }
 
-// Lax-Friedrichs split of stencil cell s (reference semantics: alpha = 3):
-// fL = (F + alpha U)/2 for s = 0..4, fR = (F - alpha U)/2 for s = 1..5; the
-// face average of W is taken from cells 2 and 3.
+// Lax-Friedrichs split of stencil cell s with halpha = alpha/2 (reference
+// semantics: alpha = 3): fL = (F + alpha U)/2 for s = 0..4, fR = (F - alpha U)/2
+// for s = 1..5; the face average of W is taken from cells 2 and 3.
 template <int DIR, bool CHAR, typename T>
 __device__ __forceinline__ void split_cell(int s, const T w[5], const T u[5], T hg, T fL[5][5],
-                                           T fR[5][5], T wa[5]) {
-    const T halpha = T(1.5), half = T(0.5);
+                                           T fR[5][5], T wa[5], T halpha = T(1.5)) {
+    const T half = T(0.5);
     if constexpr (CHAR) {
         if (s == 2) {
 #pragma unroll
@@ -184,34 +184,25 @@ __device__ __forceinline__ void face_stencil_from(Loader ld, const Consts& c, T 
             split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
         }
     } else {
-        // local Lax-Friedrichs speed max(|qn|+c) over the 6-cell stencil: the split
-        // waits until every cell's speed is known
-        T Fc[6][5], Uc[6][5], halpha = T(0);
+        // local Lax-Friedrichs speed max(|q_n| + c) over the 6-cell stencil, in a first
+        // pass over the stencil (the second pass reloads its cells from L1), with
+        // c = sqrt(gamma p/rho) = gamma p rsqrt(gamma p rho)
+        T amax = T(0);
 #pragma unroll
         for (int s = 0; s < 6; s++) {
-            T w[5];
-            ld(s, w, Uc[s]);
-            if constexpr (CHAR) {
-                if (s == 2) {
-#pragma unroll
-                    for (int q = 0; q < 5; q++) wa[q] = w[q];
-                }
-                if (s == 3) {
-#pragma unroll
-                    for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + w[q]);
-                }
-            }
-            half_flux<DIR, T>(w, hg, Fc[s]);
-            T a = half * (fabs(w[2 + DIR]) + tsqrt(gamma * w[1] * trcp(w[0])));
-            halpha = (s == 0) ? a : (a > halpha ? a : halpha);
+            T w[5], u[5];
+            ld(s, w, u);
+            const T gp = gamma * w[1];
+            const T a = fabs(w[2 + DIR]) + gp * trsqrt(gp * w[0]);
+            amax = (s == 0) ? a : (a > amax ? a : amax);
         }
+        const T halpha = half * amax;
 #pragma unroll
-        for (int s = 0; s < 6; s++)
-#pragma unroll
-            for (int q = 0; q < 5; q++) {
-                if (s <= 4) fL[q][s] = halpha * Uc[s][q] + Fc[s][q];
-                if (s >= 1) fR[q][s - 1] = Fc[s][q] - halpha * Uc[s][q];
-            }
+        for (int s = 0; s < 6; s++) {
+            T w[5], u[5];
+            ld(s, w, u);
+            split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa, halpha);
+        }
     }
 }
 

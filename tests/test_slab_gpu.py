@@ -91,7 +91,7 @@ def test_gpu_slabs_equal_the_single_domain(oracle, tmp_path, shape, world, bc, c
         assert (err[:4] <= 1e-12).all(), f"slabs vs oracle: rel L2 per field {err}"
 
 
-def _nccl_single_rank(port, pbytes, W_global, nsteps, outdir):
+def _nccl_single_rank(rank, port, pbytes, W_global, nsteps, outdir):
     import datetime
     import torch
     import torch.distributed as dist
