@@ -193,8 +193,12 @@ def test_gated_form_gains_over_component_wise(tmp_path):
 @pytest.mark.parametrize("order,weights,bc", [(2, 0, (N, P, P)), (4, 1, (P, N, P)), (6, 0, (N, N, N))])
 def test_gate_extremes_equal_the_ungated_forms(order, weights, bc):
     """A network whose only nonzero parameter is the output bias flags every face
-    (b3 > 0) or none (b3 < 0): the gated stage kernel then reproduces ungated FP32
-    characteristic-wise / component-wise on every viscous order and weight type."""
+    (b3 > 0) or none (b3 < 0).  None: the gated step is the component-wise stage
+    alone, bit for bit.  Every face: component-wise stages corrected by the
+    characteristic-wise minus component-wise flux of every face, which is FP32
+    characteristic-wise up to the FP32 rounding of that difference: as close to
+    the FP64 characteristic-wise run as ungated FP32 characteristic-wise is (to
+    10 %), and within 5e-6 of it (measured 1.4e-6 in rhoW, 2e-7 in rho)."""
     shape = (20, 12, 10)
     kw = dict(convection=pkg.CONV_WENO5_CHAR, diffusion_order=order, weights=weights, bc=bc, mu=0.02,
               cfl=0.3, precision=pkg.PREC_FP32)
@@ -212,12 +216,15 @@ def test_gate_extremes_equal_the_ungated_forms(order, weights, bc):
             s.advance(3)
             return s.download_conservative(), s.diagnostics()["sensor_fraction"]
 
+    U_64, _ = run(precision=pkg.PREC_FP64)
     U_char, _ = run()
     U_comp, _ = run(convection=pkg.CONV_WENO5)
     U_all, f_all = run(sensor=1, b3=10.0)
     U_none, f_none = run(sensor=1, b3=-10.0)
     assert f_all == 1.0 and f_none == 0.0
+    np.testing.assert_array_equal(interior(U_none), interior(U_comp))
     e_all = rel_l2(interior(U_all), interior(U_char))
-    e_none = rel_l2(interior(U_none), interior(U_comp))
-    assert (e_all <= 1e-6).all(), f"all flagged vs characteristic-wise: {e_all}"
-    assert (e_none <= 1e-6).all(), f"none flagged vs component-wise: {e_none}"
+    assert (e_all <= 5e-6).all(), f"all flagged vs characteristic-wise: {e_all}"
+    acc_all = rel_l2(interior(U_all), interior(U_64))
+    acc_char = rel_l2(interior(U_char), interior(U_64))
+    assert (acc_all <= 1.1 * acc_char).all(), (acc_all, acc_char)
