@@ -821,6 +821,8 @@ ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time) {
 ns_status ns_synchronize(ns_ctx* ctx) {
     if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
     NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (ctx->sensor && sensor_status(ctx->sensor) != NS_OK)
+        return fail(NS_ERR_TIMEOUT, "a tensor-core wait of the sensor's flag kernel ran out of polls");
     return check_state(ctx);
 }
 

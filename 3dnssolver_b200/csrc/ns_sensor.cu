@@ -38,6 +38,7 @@
 #include "ns_eos.cuh"
 #include "ns_face.cuh"
 #include "ns_sensor.h"
+#include "ns_tcgen05.cuh"
 
 namespace nsb {
 
@@ -46,6 +47,14 @@ constexpr int SH = 32;                  // hidden width
 constexpr int SP = NS_SENSOR_NPARAMS;   // 2145
 constexpr int OFF_W1 = 0, OFF_B1 = 1024, OFF_W2 = 1056, OFF_B2 = 2080, OFF_W3 = 2112, OFF_B3 = 2144;
 constexpr int XS = 40;  // bf16 row stride of the smem tiles (conflict-free fragment loads)
+
+// The per-step flags run the network on the 5th-generation tensor cores
+// (tcgen05.mma, TMEM accumulators) unless built with NS_SENSOR_TCGEN05=0, which
+// selects the warp-level mma.sync kernel (training and ns_sensor_predict always
+// use mma.sync).
+#ifndef NS_SENSOR_TCGEN05
+#define NS_SENSOR_TCGEN05 1
+#endif
 
 // ---------------------------------------------------------------------------
 // tensor-core building blocks
@@ -799,6 +808,173 @@ __global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ p
     if (lane == 0 && nfire) atomicAdd(flagged, nfire);
 }
 
+// The same flags on the 5th-generation tensor cores: a CTA of 128 threads takes
+// 128 faces per tile; their BF16 features (K = 32, the 21 features and zeros)
+// and the network's weight tiles sit in shared memory in the K-major layout, one
+// thread issues two K = 16 tcgen05.mma per layer (M = 128 faces, N = 32 hidden
+// units, FP32 accumulators in 32 TMEM columns) and commits them to an
+// mbarrier, and every thread reads its face's 32 pre-activations back with
+// tcgen05.ld for the bias, the GELU and the next layer's operand.  A wait that
+// runs out of polls sets *err and ends the kernel after freeing its TMEM.
+constexpr uint32_t kMmaPolls = 1u << 24;
+
+template <int DIR>
+__global__ void __launch_bounds__(128) k_sensor_mask_tc(const float* __restrict__ prim, Box b, Consts c,
+                                                        FaceBox fb, const float* __restrict__ w,
+                                                        float logit_thr, unsigned char* __restrict__ mask,
+                                                        unsigned long long* __restrict__ flagged,
+                                                        unsigned* __restrict__ list, unsigned* __restrict__ count,
+                                                        unsigned char* __restrict__ touched, int* __restrict__ err) {
+    __shared__ __align__(128) unsigned char A1[128 * 32 * 2];
+    __shared__ __align__(128) unsigned char A2[128 * 32 * 2];
+    __shared__ __align__(128) unsigned char B1[32 * 32 * 2];
+    __shared__ __align__(128) unsigned char B2[32 * 32 * 2];
+    __shared__ float vb1[SH], vb2[SH], vw3[SH];
+    __shared__ float vb3;
+    __shared__ __align__(8) unsigned long long bar;
+    __shared__ uint32_t tslot;
+    const int warp = threadIdx.y, lane = threadIdx.x, tid = warp * 32 + lane;
+    // weight tiles [n][k] in the K-major layout (W1's columns past the 21 features are zero)
+    for (int e = tid; e < SH * 32; e += 128) {
+        const int n = e >> 5, k = e & 31;
+        *reinterpret_cast<__nv_bfloat16*>(B1 + tc::kmajor_offset<32>(n, k)) =
+            __float2bfloat16(k < SF ? w[OFF_W1 + n * 32 + k] : 0.f);
+        *reinterpret_cast<__nv_bfloat16*>(B2 + tc::kmajor_offset<32>(n, k)) = __float2bfloat16(w[OFF_W2 + n * 32 + k]);
+    }
+    if (tid < SH) {
+        vb1[tid] = w[OFF_B1 + tid];
+        vb2[tid] = w[OFF_B2 + tid];
+        vw3[tid] = w[OFF_W3 + tid];
+    }
+    if (tid == 0) vb3 = w[OFF_B3];
+    const uint32_t bar_a = tc::smem_u32(&bar);
+    if (tid == 0) tc::mbar_init(bar_a, 1);
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&tslot), 32);
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+    constexpr uint32_t idesc = tc::idesc_bf16_f32<128, 32>();
+    // K halves: A tiles (128 rows) 2 x 2048 B apart, B tiles (32 rows) 2 x 512 B apart
+    const uint64_t dA1[2] = {tc::kmajor_desc(tc::smem_u32(A1), 2048, 128), tc::kmajor_desc(tc::smem_u32(A1) + 4096, 2048, 128)};
+    const uint64_t dA2[2] = {tc::kmajor_desc(tc::smem_u32(A2), 2048, 128), tc::kmajor_desc(tc::smem_u32(A2) + 4096, 2048, 128)};
+    const uint64_t dB1[2] = {tc::kmajor_desc(tc::smem_u32(B1), 512, 128), tc::kmajor_desc(tc::smem_u32(B1) + 1024, 512, 128)};
+    const uint64_t dB2[2] = {tc::kmajor_desc(tc::smem_u32(B2), 512, 128), tc::kmajor_desc(tc::smem_u32(B2) + 1024, 512, 128)};
+    const float gamma = float(c.gamma);
+    const unsigned t2 = (fb.n2 + 31) / 32, t1 = (fb.n1 + 3) / 4, t12 = t2 * t1;
+    const unsigned tiles = t12 * (unsigned)fb.n0;
+    const long long n = (long long)b.nx * b.ny * b.nz;
+    uint32_t phase = 0;
+    bool ok = true;
+    unsigned long long nfire = 0;
+    for (unsigned t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const unsigned aa_ = t / t12, r = t - aa_ * t12, b1 = r / t2;
+        const int kk = (int)(r - b1 * t2) * 32 + lane;
+        const int bb = (int)b1 * 4 + warp;
+        const int aa = (int)aa_;
+        const bool live = kk < fb.n2 && bb < fb.n1;
+        float feat[32];
+#pragma unroll
+        for (int e = 0; e < 32; e++) feat[e] = 0.f;
+        if (live) {
+            float rho[6], p[6], un[6];
+#pragma unroll
+            for (int s = 0; s < 6; s++) {
+                int i = aa, j = bb, k = kk;
+                if (DIR == 0) i = fold(aa - 3 + s, b.nx, c.periodic[0]);
+                if (DIR == 1) j = fold(bb - 3 + s, b.ny, c.periodic[1]);
+                if (DIR == 2) k = fold(kk - 3 + s, b.nz, c.periodic[2]);
+                const long long e = ((long long)i * b.ny + j) * b.nz + k;
+                rho[s] = prim[e];
+                p[s] = prim[n + e];
+                un[s] = prim[(2 + DIR) * n + e];
+            }
+            face_features<float>(rho, p, un, gamma, feat);
+        }
+        // this face is row tid of the A tile: four 16-byte chunks of 8 features
+#pragma unroll
+        for (int kb = 0; kb < 4; kb++) {
+            uint32_t q[4];
+#pragma unroll
+            for (int h = 0; h < 4; h++) q[h] = pack_bf16(feat[8 * kb + 2 * h], feat[8 * kb + 2 * h + 1]);
+            *reinterpret_cast<uint4*>(A1 + tc::kmajor_offset<128>(tid, 8 * kb)) = make_uint4(q[0], q[1], q[2], q[3]);
+        }
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) {
+            tc::mma_bf16(tmem, dA1[0], dB1[0], idesc, false);
+            tc::mma_bf16(tmem, dA1[1], dB1[1], idesc, true);
+            tc::commit_to(bar_a);
+        }
+        ok = tc::mbar_wait(bar_a, phase, kMmaPolls) && ok;
+        phase ^= 1;
+        tc::fence_after_sync();
+        float d[32];
+        tc::tmem_ld32(trow, d);
+        // layer 1: GELU(z + b1) as the second layer's BF16 operand, row tid
+#pragma unroll
+        for (int kb = 0; kb < 4; kb++) {
+            uint32_t q[4];
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const int e = 8 * kb + 2 * h;
+                __nv_bfloat162 v = gelu_bf16x2(d[e] + vb1[e], d[e + 1] + vb1[e + 1]);
+                q[h] = *reinterpret_cast<uint32_t*>(&v);
+            }
+            *reinterpret_cast<uint4*>(A2 + tc::kmajor_offset<128>(tid, 8 * kb)) = make_uint4(q[0], q[1], q[2], q[3]);
+        }
+        tc::fence_smem_to_async();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) {
+            tc::mma_bf16(tmem, dA2[0], dB2[0], idesc, false);
+            tc::mma_bf16(tmem, dA2[1], dB2[1], idesc, true);
+            tc::commit_to(bar_a);
+        }
+        ok = tc::mbar_wait(bar_a, phase, kMmaPolls) && ok;
+        phase ^= 1;
+        tc::fence_after_sync();
+        tc::tmem_ld32(trow, d);
+        float lg = vb3;
+#pragma unroll
+        for (int e = 0; e < 32; e += 2) {
+            const float2 g = __bfloat1622float2(gelu_bf16x2(d[e] + vb2[e], d[e + 1] + vb2[e + 1]));
+            lg = fmaf(g.x, vw3[e], fmaf(g.y, vw3[e + 1], lg));
+        }
+        const bool fire = live && lg > logit_thr;
+        const long long fi = live ? fb.at(aa, bb, kk) : 0;
+        if (live) mask[fi] = fire ? 1 : 0;
+        const unsigned m = __ballot_sync(0xffffffffu, fire);
+        nfire += __popc(m);
+        if (m) {
+            unsigned base = 0;
+            if (lane == 0) base = atomicAdd(count, (unsigned)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (fire) {
+                list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)fi;
+                const int a = DIR == 0 ? aa : (DIR == 1 ? bb : kk), na = DIR == 0 ? b.nx : (DIR == 1 ? b.ny : b.nz);
+                const long long cell = ((long long)aa * b.ny + bb) * b.nz + kk;
+                const long long step = DIR == 0 ? (long long)b.ny * b.nz : (DIR == 1 ? (long long)b.nz : 1LL);
+                if (a - 1 >= 0) touched[cell - step] = 1;
+                if (a < na) touched[cell] = 1;
+            }
+        }
+        tc::fence_before_sync();  // this tile's TMEM reads precede the next tile's MMA
+        if (!__syncthreads_and(ok)) break;
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    if (lane == 0 && nfire) atomicAdd(flagged, nfire);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_free(tmem, 32);
+}
+
 // compacted list of the touched cells (interior order), the cells a correction pass updates
 __global__ void __launch_bounds__(128) k_sensor_touched_list(const unsigned char* __restrict__ touched, long long n,
                                                              unsigned* __restrict__ list, unsigned* __restrict__ count) {
@@ -825,6 +1001,7 @@ struct SensorState {
     unsigned char* touched = nullptr;      // cells next to a flagged face, one byte per interior cell
     unsigned* cells = nullptr;             // the touched cells (compacted)
     long long ncells = 0;
+    int* err = nullptr;                    // set by a tensor-core wait that ran out of polls
     float* prim = nullptr;                  // the step's rho, p, u, v, w (FP32 planes) for the flags
     unsigned long long faces = 0;           // faces evaluated since creation (host count)
     int sms = 148;                          // multiprocessors of the context's device
@@ -841,7 +1018,8 @@ ns_status sensor_create(SensorState** out, const Box& b, const FaceBox* fb, cuda
     for (int d = 0; d < 3 && ok; d++)
         ok = cudaMalloc(&st->list[d], (size_t)fb[d].fstride * sizeof(unsigned)) == cudaSuccess;
     st->ncells = (long long)b.nx * b.ny * b.nz;
-    ok = ok && cudaMalloc(&st->counts, 4 * sizeof(unsigned)) == cudaSuccess &&
+    ok = ok && cudaMalloc(&st->err, sizeof(int)) == cudaSuccess &&
+         cudaMalloc(&st->counts, 4 * sizeof(unsigned)) == cudaSuccess &&
          cudaMalloc(&st->touched, (size_t)st->ncells) == cudaSuccess &&
          cudaMalloc(&st->cells, (size_t)st->ncells * sizeof(unsigned)) == cudaSuccess;
     ok = ok && cudaMalloc(&st->prim, (size_t)5 * b.nx * b.ny * b.nz * sizeof(float)) == cudaSuccess;
@@ -856,6 +1034,7 @@ ns_status sensor_create(SensorState** out, const Box& b, const FaceBox* fb, cuda
     cudaMemsetAsync(st->w, 0, SP * sizeof(float), s);
     cudaMemsetAsync(st->flagged, 0, sizeof(unsigned long long), s);
     cudaMemsetAsync(st->counts, 0, 4 * sizeof(unsigned), s);
+    cudaMemsetAsync(st->err, 0, sizeof(int), s);
     *out = st;
     return NS_OK;
 }
@@ -867,6 +1046,7 @@ void sensor_destroy(SensorState* st) {
     for (int d = 0; d < 3; d++) cudaFree(st->mask[d]);
     for (int d = 0; d < 3; d++) cudaFree(st->list[d]);
     cudaFree(st->counts);
+    cudaFree(st->err);
     cudaFree(st->touched);
     cudaFree(st->cells);
     cudaFree(st->prim);
@@ -922,16 +1102,19 @@ ns_status sensor_step_flags(SensorState* st, const double* U0, const Box& b, con
         const FaceBox& f = fb[d];
         const long long tiles = (long long)((f.n2 + 31) / 32) * ((f.n1 + 3) / 4) * f.n0;
         if (tiles >= (1ll << 31) || f.fstride >= (1ll << 32)) return NS_ERR_UNSUPPORTED;
+#if NS_SENSOR_TCGEN05
+        const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 8);
+#define NS_MASK(D) k_sensor_mask_tc<D><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[D], st->flagged, \
+                                                          st->list[D], st->counts + D, st->touched, st->err)
+#else
         const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
-        if (d == 0)
-            k_sensor_mask<0><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[0], st->flagged, st->list[0],
-                                                st->counts + 0, st->touched);
-        else if (d == 1)
-            k_sensor_mask<1><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[1], st->flagged, st->list[1],
-                                                st->counts + 1, st->touched);
-        else
-            k_sensor_mask<2><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[2], st->flagged, st->list[2],
-                                                st->counts + 2, st->touched);
+#define NS_MASK(D) k_sensor_mask<D><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[D], st->flagged, \
+                                                       st->list[D], st->counts + D, st->touched)
+#endif
+        if (d == 0) NS_MASK(0);
+        else if (d == 1) NS_MASK(1);
+        else NS_MASK(2);
+#undef NS_MASK
         st->faces += (unsigned long long)f.n0 * f.n1 * f.n2;
         if (launches) (*launches)++;
     }
@@ -939,6 +1122,12 @@ ns_status sensor_step_flags(SensorState* st, const double* U0, const Box& b, con
                                                                               st->counts + 3);
     if (launches) (*launches)++;
     return cudaGetLastError() == cudaSuccess ? NS_OK : NS_ERR_CUDA;
+}
+
+ns_status sensor_status(SensorState* st) {
+    int e = 0;
+    if (cudaMemcpy(&e, st->err, sizeof e, cudaMemcpyDeviceToHost) != cudaSuccess) return NS_ERR_CUDA;
+    return e ? NS_ERR_TIMEOUT : NS_OK;
 }
 
 GateLists sensor_gate_lists(const SensorState* st) {

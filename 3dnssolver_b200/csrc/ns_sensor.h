@@ -24,6 +24,8 @@ ns_status sensor_face_flux(SensorState* st, int dir, const double* W, const doub
 ns_status sensor_step_flags(SensorState* st, const double* U0, const Box& b, const Consts& c, double threshold,
                             const FaceBox fb[3], int conv_dims, cudaStream_t s, long long* launches);
 GateLists sensor_gate_lists(const SensorState* st);
+// NS_ERR_TIMEOUT if a tensor-core wait of the flag kernels ran out of polls (waits for the device)
+ns_status sensor_status(SensorState* st);
 // fraction of evaluated faces the sensor flagged since the context was created
 double sensor_last_fraction(SensorState* st);
 ns_status sensor_set_weights(SensorState* st, const float* w, cudaStream_t s);

@@ -228,3 +228,33 @@ def test_gate_extremes_equal_the_ungated_forms(order, weights, bc):
     acc_all = rel_l2(interior(U_all), interior(U_64))
     acc_char = rel_l2(interior(U_char), interior(U_64))
     assert (acc_all <= 1.1 * acc_char).all(), (acc_all, acc_char)
+
+
+@pytest.mark.gpu
+def test_step_flags_agree_with_the_predict_path():
+    """The per-step flags (the network on the tcgen05 tensor cores, from the step's
+    FP32 primitive planes) flag the same faces, up to the last BF16 rounding, as
+    ns_sensor_predict (mma.sync) on the features harvested from the same state."""
+    import torch
+    sensor_mod = importlib.import_module("3dnssolver_b200.sensor")
+    X, y = sensor_mod.default_training_set()
+    w, _ = sensor_mod.train(X, y, seed=3)
+    p32 = _sod_params(96, 12, 12, precision=pkg.PREC_FP32, sensor=1)
+    W0 = wl.sod(p32, seed=3)
+    with pkg.Solver(p32) as s:
+        s.set_sensor_weights(w)
+        s.upload_primitive(W0)
+        s.advance(1)
+        frac_step = s.diagnostics()["sensor_fraction"]
+    p64 = _sod_params(96, 12, 12)
+    with pkg.Solver(p64) as s:
+        s.upload_primitive(W0)
+        cap = s.faces()
+        f = torch.empty((cap, pkg.SENSOR_FEATURES), dtype=torch.float32, device="cuda")
+        lab = torch.empty(cap, dtype=torch.float32, device="cuda")
+        n = s.sensor_harvest(f.data_ptr(), lab.data_ptr(), cap)
+    lg = torch.empty(n, dtype=torch.float32, device="cuda")
+    pkg.sensor_predict(f.data_ptr(), n, w, lg.data_ptr())
+    frac_pred = float((lg > 0).float().mean().item())
+    assert frac_pred > 0.01
+    assert abs(frac_step - frac_pred) <= 0.005 + 0.02 * frac_pred, (frac_step, frac_pred)
