@@ -39,8 +39,6 @@
 
 namespace nsb {
 
-constexpr int FT = 256;  // threads per block
-
 // ---------------------------------------------------------------------------
 // A block marches LX cells along x over a TY x TZ column: 2.2 plane loads per
 // cell (a 3D box tile with the same shared memory needed 7.4 and ran 20%
@@ -60,15 +58,20 @@ constexpr int FT = 256;  // threads per block
 // between planes, so a plane needs two block barriers instead of three: the
 // next plane's conversion overwrites plane i-2, whose last reader (the x-faces)
 // finished before this plane's second barrier.
+//
+// FP64 (the plain form's fused stage) uses an 8 x 16 column and 128 threads:
+// its ring of 6 FP64 planes and face buffers then take 109 KB, so two blocks
+// fit on an SM and each thread has up to 255 registers for the FP64 face code.
 template <typename T, int H = 1>
 struct MarchTile {
-    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = 32;
+    static constexpr int TY = NS_MARCH_TY, TZ = sizeof(T) == 8 ? 16 : 32, LX = 32;
+    static constexpr int FT = TY * TZ;  // threads per block, one per cell of the column
     static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
     static constexpr bool LEAN = H <= 1;
     static constexpr int RING = LEAN ? 6 : 7;
     static constexpr int NBUF = LEAN ? 2 : 1;
     static constexpr int NFY = (TY + 1) * TZ, NFZ = TY * (TZ + 1);
-    static constexpr int MINB = sizeof(T) == 8 ? 1 : 2;
+    static constexpr int MINB = 2;
     // ring, y/z face buffers, and the FP64 conserved state of the plane in flight
     static constexpr size_t smem = (size_t)RING * 5 * NP * sizeof(T) +
                                    (size_t)NBUF * 5 * (NFY + NFZ) * sizeof(T) + (size_t)5 * NP * sizeof(double);
@@ -79,42 +82,39 @@ struct MarchTile {
 // pass: the partial last round of each pass (plane loads, y-faces, z-faces)
 // then falls to a different warp instead of piling up on warp 0 before the
 // same barrier.
-__device__ __forceinline__ int rotated(int tid, int w) { return (tid + FT - 32 * w) % FT; }
+template <int FT>
+__device__ __forceinline__ int rotated(int tid, int w) { return (tid + FT - (32 * w) % FT) % FT; }
 
 template <int RING>
 __device__ __forceinline__ int ring_slot(int i, int x0) {
     return (i - x0 + 3) % RING;  // i >= x0 - 3
 }
 
-// one face from a 6-cell stencil in a shared array with stride `step`
+// one face from a 6-cell stencil in a shared array with stride `step`; FP64
+// forms U = cons(W) with the equation of state's explicit roundings, as the
+// unfused W-only face kernels do
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T>
-__device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, T gamma,
-                                           T inv_gm1, T out[5]) {
+__device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, const Consts& c,
+                                           T out[5]) {
+    const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
     if constexpr (sizeof(T) == 4) {
         face_f32x2<DIR, CHAR, BORGES, PHYS>(planes, c0, step, fs, gamma, inv_gm1, out);
         return;
-    }
-    static_assert(sizeof(T) == 4 || !PHYS, "the FP64 march face follows the reference semantics");
-    const T hg = T(0.5) * gamma * inv_gm1;
-    T fL[5][5], fR[5][5], wa[5];
+    } else {
+        auto ld = [&](int s, double w[5], double u[5]) {
+            const T* P = planes[s];
+            const int idx = c0 + s * step;
 #pragma unroll
-    for (int s = 0; s < 6; s++) {
-        const T* P = planes[s];
-        int idx = c0 + s * step;
-        T w[5], u[5];
-#pragma unroll
-        for (int q = 0; q < 5; q++) w[q] = P[q * fs + idx];
-        u[0] = w[0];
-        u[2] = w[0] * w[2];
-        u[3] = w[0] * w[3];
-        u[4] = w[0] * w[4];
-        u[1] = w[1] * inv_gm1 + T(0.5) * w[0] * (w[2] * w[2] + w[3] * w[3] + w[4] * w[4]);
-        split_cell<DIR, CHAR, T>(s, w, u, hg, fL, fR, wa);
+            for (int q = 0; q < 5; q++) w[q] = P[q * fs + idx];
+            cons_from_prim(w, c.inv_gm1, u);
+        };
+        double fL[5][5], fR[5][5], wa[5];
+        face_stencil_from<DIR, CHAR, PHYS, double>(ld, c, fL, fR, wa);
+        if constexpr (CHAR)
+            face_char<DIR, PHYS, double, BORGES>(fL, fR, wa, c.gamma, c.inv_gm1, out);
+        else
+            face_comp<double, BORGES>(fL, fR, out);
     }
-    if constexpr (CHAR)
-        face_char<DIR, false, T, BORGES>(fL, fR, wa, gamma, inv_gm1, out);
-    else
-        face_comp<T, BORGES>(fL, fR, out);
 }
 
 
@@ -266,12 +266,13 @@ __device__ __forceinline__ void march_viscous_physical(PlaneFn plane, int i, int
 }
 
 template <typename T, bool CHAR, bool BORGES, int H, bool LAST, bool PHYS>
-__global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
+__global__ void __launch_bounds__(MarchTile<T, H>::FT, MarchTile<T, H>::MINB)
     k_stage_march(const double* __restrict__ Uin, double* U0, double* __restrict__ Uout, Box b,
                   Consts c, int conv_dims, double m1, double m2, double mc,
                   const unsigned long long* __restrict__ slot, unsigned long long* slot_next,
                   double* clock, const unsigned char* __restrict__ skip) {
     using M = MarchTile<T, H>;
+    constexpr int FT = M::FT;
     static_assert(M::NFY <= 2 * FT && M::NFZ <= 2 * FT, "a face pass takes at most two rounds");
     extern __shared__ __align__(16) unsigned char smem[];
     T* ring = reinterpret_cast<T*>(smem);        // [RING][5][NP]
@@ -281,13 +282,12 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     const int tid = threadIdx.x, ty = tid / M::TZ, tz = tid % M::TZ;
     const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * M::LX;
     const int x1 = min(x0 + M::LX, b.nx);
-    const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
     auto plane = [&](int i) { return ring + ring_slot<M::RING>(i, x0) * 5 * M::NP; };
     // U_in of plane i at folded positions, into S without waiting (each thread
     // later converts exactly the elements it copied, so S needs no barrier)
     auto issue_plane = [&](int i) {
         const int gi = fold_x(i, b.nx, c);
-        for (int e = rotated(tid, 5); e < M::NP; e += FT) {
+        for (int e = rotated<FT>(tid, 5); e < M::NP; e += FT) {
             int py = e / M::PZ, pz = e % M::PZ;
             int gj = fold(j0 - 3 + py, b.ny, c.periodic[1]);
             int gk = fold(k0 - 3 + pz, b.nz, c.periodic[2]);
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
     auto convert_plane = [&](int i) {
         cp_async_wait_all();
         T* P = plane(i);
-        for (int e = rotated(tid, 5); e < M::NP; e += FT) {
+        for (int e = rotated<FT>(tid, 5); e < M::NP; e += FT) {
             if constexpr (sizeof(T) == 4) {
                 // the FP32 form's W in FP32 arithmetic from the FP64 state
                 float u[5];
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
         const T* P[6];
 #pragma unroll
         for (int s = 0; s < 6; s++) P[s] = plane(i - 2 + s);
-        march_face<0, CHAR, BORGES, PHYS, T>(P, ccol, 0, M::NP, gamma, inv_gm1, out);
+        march_face<0, CHAR, BORGES, PHYS, T>(P, ccol, 0, M::NP, c, out);
     };
     const int gj = j0 + ty, gk = k0 + tz;
     const bool row = ty < M::TY;  // the eighth warp only helps with the y- and z-faces
@@ -362,20 +362,20 @@ __global__ void __launch_bounds__(FT, MarchTile<T, H>::MINB)
         if (conv_dims > 0) {
             if (row) xface(i, fxr);
             // y-faces of plane i: between rows fb-1 and fb, stencil rows fb..fb+5 of the plane
-            for (int e = rotated(tid, 7); e < M::NFY; e += FT) {
+            for (int e = rotated<FT>(tid, 7); e < M::NFY; e += FT) {
                 int fb = e / M::TZ, cz = e % M::TZ;
                 const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                 T out[5];
-                march_face<1, CHAR, BORGES, PHYS, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, gamma, inv_gm1, out);
+                march_face<1, CHAR, BORGES, PHYS, T>(P, fb * M::PZ + cz + 3, M::PZ, M::NP, c, out);
 #pragma unroll
                 for (int q = 0; q < 5; q++) FY[q * M::NFY + e] = out[q];
             }
             if (conv_dims == 3) {
-                for (int e = rotated(tid, 6); e < M::NFZ; e += FT) {
+                for (int e = rotated<FT>(tid, 6); e < M::NFZ; e += FT) {
                     int ry = e / (M::TZ + 1), fc = e % (M::TZ + 1);
                     const T* P[6] = {Pi, Pi, Pi, Pi, Pi, Pi};
                     T out[5];
-                    march_face<2, CHAR, BORGES, PHYS, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, gamma, inv_gm1, out);
+                    march_face<2, CHAR, BORGES, PHYS, T>(P, (ry + 3) * M::PZ + fc, 1, M::NP, c, out);
 #pragma unroll
                     for (int q = 0; q < 5; q++) FZ[q * M::NFZ + e] = out[q];
                 }
@@ -443,35 +443,38 @@ static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
     if (e != cudaSuccess) return e;
     dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + M::LX - 1) / M::LX);
-    kern<<<grid, FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
+    kern<<<grid, M::FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
                                    a.slot_next, a.clock, a.skip);
     return cudaGetLastError();
 }
 
-template <bool PHYS, bool CHAR, bool BORGES, bool LAST>
+template <typename T, bool PHYS, bool CHAR, bool BORGES, bool LAST>
 static cudaError_t fused_h(const FusedArgs& a, cudaStream_t s) {
     switch (a.visc_h) {
-        case 0: return fused_one<float, CHAR, BORGES, 0, LAST, PHYS>(a, s);
-        case 1: return fused_one<float, CHAR, BORGES, 1, LAST, PHYS>(a, s);
-        case 2: return fused_one<float, CHAR, BORGES, 2, LAST, PHYS>(a, s);
-        default: return fused_one<float, CHAR, BORGES, 3, LAST, PHYS>(a, s);
+        case 0: return fused_one<T, CHAR, BORGES, 0, LAST, PHYS>(a, s);
+        case 1: return fused_one<T, CHAR, BORGES, 1, LAST, PHYS>(a, s);
+        case 2: return fused_one<T, CHAR, BORGES, 2, LAST, PHYS>(a, s);
+        default: return fused_one<T, CHAR, BORGES, 3, LAST, PHYS>(a, s);
     }
 }
 
-// One fused FP32 stage of the given semantics (instantiated in ns_fused_ref.cu
-// and ns_fused_phys.cu).
-template <bool PHYS>
+// One fused stage in arithmetic T of the given semantics (instantiated per
+// type and semantics in ns_fused_{ref,phys}{,64}.cu).
+template <typename T, bool PHYS>
 cudaError_t fused_launch(const FusedArgs& a, cudaStream_t s) {
-    if (!a.fp32) return cudaErrorInvalidValue;  // the FP32 form only
+    if (a.fp32 != (sizeof(T) == 4)) return cudaErrorInvalidValue;
     if (a.chr) {
-        if (a.borges) return a.last ? fused_h<PHYS, true, true, true>(a, s) : fused_h<PHYS, true, true, false>(a, s);
-        return a.last ? fused_h<PHYS, true, false, true>(a, s) : fused_h<PHYS, true, false, false>(a, s);
+        if (a.borges)
+            return a.last ? fused_h<T, PHYS, true, true, true>(a, s) : fused_h<T, PHYS, true, true, false>(a, s);
+        return a.last ? fused_h<T, PHYS, true, false, true>(a, s) : fused_h<T, PHYS, true, false, false>(a, s);
     }
-    if (a.borges) return a.last ? fused_h<PHYS, false, true, true>(a, s) : fused_h<PHYS, false, true, false>(a, s);
-    return a.last ? fused_h<PHYS, false, false, true>(a, s) : fused_h<PHYS, false, false, false>(a, s);
+    if (a.borges) return a.last ? fused_h<T, PHYS, false, true, true>(a, s) : fused_h<T, PHYS, false, true, false>(a, s);
+    return a.last ? fused_h<T, PHYS, false, false, true>(a, s) : fused_h<T, PHYS, false, false, false>(a, s);
 }
 
-extern template cudaError_t fused_launch<false>(const FusedArgs& a, cudaStream_t s);
-extern template cudaError_t fused_launch<true>(const FusedArgs& a, cudaStream_t s);
+extern template cudaError_t fused_launch<float, false>(const FusedArgs& a, cudaStream_t s);
+extern template cudaError_t fused_launch<float, true>(const FusedArgs& a, cudaStream_t s);
+extern template cudaError_t fused_launch<double, false>(const FusedArgs& a, cudaStream_t s);
+extern template cudaError_t fused_launch<double, true>(const FusedArgs& a, cudaStream_t s);
 
 }  // namespace nsb

@@ -2,5 +2,5 @@
 #include "ns_fused.cuh"
 
 namespace nsb {
-template cudaError_t fused_launch<true>(const FusedArgs& a, cudaStream_t s);
+template cudaError_t fused_launch<float, true>(const FusedArgs& a, cudaStream_t s);
 }  // namespace nsb
