@@ -16,12 +16,6 @@
 
 using namespace nsb;
 
-// FP64 time steps as one fused kernel per stage (8 x 16 column, ns_fused.cuh)
-// instead of the face kernels + x-face march; selected at build time.
-#ifndef NS_FP64_FUSED
-#define NS_FP64_FUSED 0
-#endif
-
 namespace {
 
 thread_local std::string g_err;
@@ -650,7 +644,7 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
     // load and compute phases with, and the FP64-pipe-bound face kernels of the
     // unfused path run faster (measured on B200 at 256^3: 2.18 vs 3.06 G
     // cell-updates/s for the characteristic scheme).
-    ctx->fused = p->precision == NS_PREC_FP32 || (NS_FP64_FUSED && p->convection != NS_CONV_NONE);
+    ctx->fused = p->precision == NS_PREC_FP32;
     ctx->xfused = !ctx->fused && p->precision == NS_PREC_FP64 && p->convection != NS_CONV_NONE;
     if (ctx->fused || ctx->xfused) A((void**)&ctx->U2, soa_bytes(ctx->box));
     if (ctx->xfused) A((void**)&ctx->W2, soa_bytes(ctx->box));

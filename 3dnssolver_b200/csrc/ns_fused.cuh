@@ -59,12 +59,16 @@ namespace nsb {
 // next plane's conversion overwrites plane i-2, whose last reader (the x-faces)
 // finished before this plane's second barrier.
 //
-// FP64 (the plain form's fused stage) uses an 8 x 16 column and 128 threads:
-// its ring of 6 FP64 planes and face buffers then take 109 KB, so two blocks
-// fit on an SM and each thread has up to 255 registers for the FP64 face code.
+// The FP32 form runs here; the FP64 form runs the face kernels and the x-face
+// march of ns_kernels.cu.  An FP64 variant of this kernel on an 8 x 16 column
+// (128 threads, 109 KB, two blocks of 252 registers per SM) reproduced the FP64
+// path's results exactly but ran 1.25-1.56x slower on B200 (Taylor-Green and
+// shear layer at 256^3): with 8 warps per SM and the plane barriers, the FP64
+// pipe idles; the separate face kernels keep it 62-67% busy at 12 warps.
 template <typename T, int H = 1>
 struct MarchTile {
-    static constexpr int TY = NS_MARCH_TY, TZ = sizeof(T) == 8 ? 16 : 32, LX = 32;
+    static_assert(sizeof(T) == 4, "the fused stage serves the FP32 form");
+    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = 32;
     static constexpr int FT = TY * TZ;  // threads per block, one per cell of the column
     static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
     static constexpr bool LEAN = H <= 1;
@@ -90,31 +94,11 @@ __device__ __forceinline__ int ring_slot(int i, int x0) {
     return (i - x0 + 3) % RING;  // i >= x0 - 3
 }
 
-// one face from a 6-cell stencil in a shared array with stride `step`; FP64
-// forms U = cons(W) with the equation of state's explicit roundings, as the
-// unfused W-only face kernels do
+// one face from a 6-cell stencil in a shared array with stride `step`
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T>
 __device__ __forceinline__ void march_face(const T* const* planes, int c0, int step, int fs, const Consts& c,
                                            T out[5]) {
-    const T gamma = T(c.gamma), inv_gm1 = T(c.inv_gm1);
-    if constexpr (sizeof(T) == 4) {
-        face_f32x2<DIR, CHAR, BORGES, PHYS>(planes, c0, step, fs, gamma, inv_gm1, out);
-        return;
-    } else {
-        auto ld = [&](int s, double w[5], double u[5]) {
-            const T* P = planes[s];
-            const int idx = c0 + s * step;
-#pragma unroll
-            for (int q = 0; q < 5; q++) w[q] = P[q * fs + idx];
-            cons_from_prim(w, c.inv_gm1, u);
-        };
-        double fL[5][5], fR[5][5], wa[5];
-        face_stencil_from<DIR, CHAR, PHYS, double>(ld, c, fL, fR, wa);
-        if constexpr (CHAR)
-            face_char<DIR, PHYS, double, BORGES>(fL, fR, wa, c.gamma, c.inv_gm1, out);
-        else
-            face_comp<double, BORGES>(fL, fR, out);
-    }
+    face_f32x2<DIR, CHAR, BORGES, PHYS>(planes, c0, step, fs, T(c.gamma), T(c.inv_gm1), out);
 }
 
 
@@ -458,11 +442,11 @@ static cudaError_t fused_h(const FusedArgs& a, cudaStream_t s) {
     }
 }
 
-// One fused stage in arithmetic T of the given semantics (instantiated per
-// type and semantics in ns_fused_{ref,phys}{,64}.cu).
+// One fused FP32 stage of the given semantics (instantiated per semantics in
+// ns_fused_{ref,phys}.cu).
 template <typename T, bool PHYS>
 cudaError_t fused_launch(const FusedArgs& a, cudaStream_t s) {
-    if (a.fp32 != (sizeof(T) == 4)) return cudaErrorInvalidValue;
+    if (!a.fp32) return cudaErrorInvalidValue;
     if (a.chr) {
         if (a.borges)
             return a.last ? fused_h<T, PHYS, true, true, true>(a, s) : fused_h<T, PHYS, true, true, false>(a, s);
@@ -474,7 +458,5 @@ cudaError_t fused_launch(const FusedArgs& a, cudaStream_t s) {
 
 extern template cudaError_t fused_launch<float, false>(const FusedArgs& a, cudaStream_t s);
 extern template cudaError_t fused_launch<float, true>(const FusedArgs& a, cudaStream_t s);
-extern template cudaError_t fused_launch<double, false>(const FusedArgs& a, cudaStream_t s);
-extern template cudaError_t fused_launch<double, true>(const FusedArgs& a, cudaStream_t s);
 
 }  // namespace nsb

@@ -145,13 +145,17 @@ static void delta_one(bool borges, const FusedArgs& a, const GateLists& L, void*
                                                            fb, (float*)F);
 }
 
+// Persistent grids sized for full residency: the delta kernel (100 registers)
+// fits 5 blocks per SM, the apply kernel (32 registers) 16; both are bound by
+// the latency of their scattered loads, so every resident warp counts.
 template <bool PHYS>
-static void gate_correct_t(const FusedArgs& a, const GateLists& L, void* const F[3], const FaceBox fb[3], int grid,
+static void gate_correct_t(const FusedArgs& a, const GateLists& L, void* const F[3], const FaceBox fb[3], int sms,
                            cudaStream_t s) {
+    const int grid_delta = sms * 5, grid = sms * 16;
     for (int d = 0; d < a.conv_dims; d++) {
-        if (d == 0) delta_one<0, PHYS>(a.borges, a, L, F[0], fb[0], grid, s);
-        else if (d == 1) delta_one<1, PHYS>(a.borges, a, L, F[1], fb[1], grid, s);
-        else delta_one<2, PHYS>(a.borges, a, L, F[2], fb[2], grid, s);
+        if (d == 0) delta_one<0, PHYS>(a.borges, a, L, F[0], fb[0], grid_delta, s);
+        else if (d == 1) delta_one<1, PHYS>(a.borges, a, L, F[1], fb[1], grid_delta, s);
+        else delta_one<2, PHYS>(a.borges, a, L, F[2], fb[2], grid_delta, s);
     }
     Gate g;
     for (int d = 0; d < 3; d++) { g.m[d] = L.mask[d]; g.fb[d] = fb[d]; }
@@ -167,9 +171,9 @@ static void gate_correct_t(const FusedArgs& a, const GateLists& L, void* const F
 
 cudaError_t gate_correct(const FusedArgs& a, const GateLists& L, void* const F[3], const FaceBox fb[3], int sms,
                          cudaStream_t s) {
-    const int grid = sms * 4;  // persistent: the list lengths stay on the device
-    if (a.phys) gate_correct_t<true>(a, L, F, fb, grid, s);
-    else gate_correct_t<false>(a, L, F, fb, grid, s);
+    // persistent: the list lengths stay on the device
+    if (a.phys) gate_correct_t<true>(a, L, F, fb, sms, s);
+    else gate_correct_t<false>(a, L, F, fb, sms, s);
     return cudaGetLastError();
 }
 

@@ -49,12 +49,10 @@ constexpr int OFF_W1 = 0, OFF_B1 = 1024, OFF_W2 = 1056, OFF_B2 = 2080, OFF_W3 = 
 constexpr int XS = 40;  // bf16 row stride of the smem tiles (conflict-free fragment loads)
 
 // The per-step flags run the network on the 5th-generation tensor cores
-// (tcgen05.mma, TMEM accumulators) unless built with NS_SENSOR_TCGEN05=0, which
-// selects the warp-level mma.sync kernel (training and ns_sensor_predict always
-// use mma.sync).
-#ifndef NS_SENSOR_TCGEN05
-#define NS_SENSOR_TCGEN05 1
-#endif
+// (tcgen05.mma, TMEM accumulators); training and ns_sensor_predict use the
+// warp-level mma.sync tiles below.  A warp-level mma.sync variant of the flag
+// kernel measured within 3% of the tcgen05 one on B200: the flag pass is bound
+// by its feature loads and GELU, not by the two small matrix products.
 
 // ---------------------------------------------------------------------------
 // tensor-core building blocks
@@ -234,64 +232,6 @@ __device__ __forceinline__ __nv_bfloat162 gelu_bf16x2(float a, float b) {
     const __nv_bfloat162 u = __hmul2(x, __hfma2(__hmul2(x, x), c1, c0));  // k0 (x + k1 x^3)
     const __nv_bfloat162 h = __hmul2(half, x);
     return __hfma2(h, tanh_bf16x2(u), h);
-}
-
-__device__ __forceinline__ void mlp_logits_fast(const MlpSmem& m, const __nv_bfloat16* X, float lg[2][2]) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-        uint32_t a[2][4];
-        afrag(X, mt, 0, g, q, a[0]);
-        afrag(X, mt, 1, g, q, a[1]);
-        float z1[4][4];
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-            float* d = z1[nt];
-            float bl = m.b1[8 * nt + 2 * q], bh = m.b1[8 * nt + 2 * q + 1];
-            d[0] = bl; d[1] = bh; d[2] = bl; d[3] = bh;
-#pragma unroll
-            for (int kt = 0; kt < 2; kt++) {
-                uint32_t b[2];
-                bfrag(m.W1, nt, kt, g, q, b);
-                mma16816(d, a[kt], b);
-            }
-        }
-        uint32_t h1a[2][4];
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-            const float* c0 = z1[2 * t];
-            const float* c1 = z1[2 * t + 1];
-            __nv_bfloat162 v;
-            v = gelu_bf16x2(c0[0], c0[1]); h1a[t][0] = *reinterpret_cast<uint32_t*>(&v);
-            v = gelu_bf16x2(c0[2], c0[3]); h1a[t][1] = *reinterpret_cast<uint32_t*>(&v);
-            v = gelu_bf16x2(c1[0], c1[1]); h1a[t][2] = *reinterpret_cast<uint32_t*>(&v);
-            v = gelu_bf16x2(c1[2], c1[3]); h1a[t][3] = *reinterpret_cast<uint32_t*>(&v);
-        }
-        float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-        for (int nt = 0; nt < 4; nt++) {
-            float d[4];
-            float bl = m.b2[8 * nt + 2 * q], bh = m.b2[8 * nt + 2 * q + 1];
-            d[0] = bl; d[1] = bh; d[2] = bl; d[3] = bh;
-#pragma unroll
-            for (int kt = 0; kt < 2; kt++) {
-                uint32_t b[2];
-                bfrag(m.W2, nt, kt, g, q, b);
-                mma16816(d, h1a[kt], b);
-            }
-            const float wl = m.w3[8 * nt + 2 * q], wh = m.w3[8 * nt + 2 * q + 1];
-            const float2 r0 = __bfloat1622float2(gelu_bf16x2(d[0], d[1]));
-            const float2 r1 = __bfloat1622float2(gelu_bf16x2(d[2], d[3]));
-            s0 = fmaf(r0.x, wl, fmaf(r0.y, wh, s0));
-            s1 = fmaf(r1.x, wl, fmaf(r1.y, wh, s1));
-        }
-        s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
-        s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
-        s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
-        lg[mt][0] = s0 + m.b3;
-        lg[mt][1] = s1 + m.b3;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -707,108 +647,10 @@ __global__ void __launch_bounds__(128) k_sensor_prims(const double* __restrict__
     prim[4 * n + e] = u[4] * ir;
 }
 
-// Flags of every face along DIR; a flagged face also goes into the compacted
-// list of its axis (FaceBox index) and marks the interior cells on either side
-// as touched, for the correction passes of ns_gate.cu.
-template <int DIR>
-__global__ void __launch_bounds__(128) k_sensor_mask(const float* __restrict__ prim, Box b, Consts c,
-                                                     FaceBox fb, const float* __restrict__ w,
-                                                     float logit_thr, unsigned char* __restrict__ mask,
-                                                     unsigned long long* __restrict__ flagged,
-                                                     unsigned* __restrict__ list, unsigned* __restrict__ count,
-                                                     unsigned char* __restrict__ touched) {
-    __shared__ __align__(16) MlpSmem m;
-    __shared__ __align__(16) __nv_bfloat16 Xs[4][32 * XS];
-    const int warp = threadIdx.y, lane = threadIdx.x;
-    mlp_load(m, w, false);  // once per block: the grid strides over 32 x 4 tiles of faces
-    __syncthreads();
-    const float gamma = float(c.gamma);
-    // tile t = (aa, tile of 4 rows, tile of 32 columns); the host keeps the
-    // tile count below 2^31
-    const unsigned t2 = (fb.n2 + 31) / 32, t1 = (fb.n1 + 3) / 4, t12 = t2 * t1;
-    const unsigned tiles = t12 * (unsigned)fb.n0;
-    const long long n = (long long)b.nx * b.ny * b.nz;
-    __nv_bfloat16* X = Xs[warp];
-    // feature columns 24..39 stay zero (K runs to 32; 21..23 are rewritten per tile)
-#pragma unroll
-    for (int e = 24; e < XS; e++) X[lane * XS + e] = __float2bfloat16(0.f);
-    unsigned long long nfire = 0;
-    for (unsigned t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const unsigned aa_ = t / t12, r = t - aa_ * t12, b1 = r / t2;
-        const int kk = (int)(r - b1 * t2) * 32 + lane;
-        const int bb = (int)b1 * 4 + warp;
-        const int aa = (int)aa_;
-        const bool live = kk < fb.n2 && bb < fb.n1;
-        float feat[24];
-        if (live) {
-            // face aa lies between cells aa-1 and aa along DIR: stencil aa-3..aa+2;
-            // rho, p and u_n in FP32 from the step's primitive planes
-            float rho[6], p[6], un[6];
-#pragma unroll
-            for (int s = 0; s < 6; s++) {
-                int i = aa, j = bb, k = kk;
-                if (DIR == 0) i = fold(aa - 3 + s, b.nx, c.periodic[0]);
-                if (DIR == 1) j = fold(bb - 3 + s, b.ny, c.periodic[1]);
-                if (DIR == 2) k = fold(kk - 3 + s, b.nz, c.periodic[2]);
-                const long long e = ((long long)i * b.ny + j) * b.nz + k;
-                rho[s] = prim[e];
-                p[s] = prim[n + e];
-                un[s] = prim[(2 + DIR) * n + e];
-            }
-            face_features<float>(rho, p, un, gamma, feat);
-        } else {
-#pragma unroll
-            for (int e = 0; e < SF; e++) feat[e] = 0.f;
-        }
-        feat[21] = feat[22] = feat[23] = 0.f;
-        __syncwarp();  // the previous tile's fragments are read
-        // three 16-byte stores per row (row stride 80 B: conflict-free per quarter warp)
-        uint4* row = reinterpret_cast<uint4*>(X + lane * XS);
-#pragma unroll
-        for (int v = 0; v < 3; v++) {
-            __nv_bfloat162 h0 = __floats2bfloat162_rn(feat[8 * v + 0], feat[8 * v + 1]);
-            __nv_bfloat162 h1 = __floats2bfloat162_rn(feat[8 * v + 2], feat[8 * v + 3]);
-            __nv_bfloat162 h2 = __floats2bfloat162_rn(feat[8 * v + 4], feat[8 * v + 5]);
-            __nv_bfloat162 h3 = __floats2bfloat162_rn(feat[8 * v + 6], feat[8 * v + 7]);
-            row[v] = make_uint4(*reinterpret_cast<uint32_t*>(&h0), *reinterpret_cast<uint32_t*>(&h1),
-                                *reinterpret_cast<uint32_t*>(&h2), *reinterpret_cast<uint32_t*>(&h3));
-        }
-        __syncwarp();
-        float lgs[2][2];
-        mlp_logits_fast(m, X, lgs);
-        float lg = 0.f;
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                float v = __shfl_sync(0xffffffffu, lgs[mt][h], 4 * (lane & 7));
-                if ((lane >> 4) == mt && ((lane >> 3) & 1) == h) lg = v;
-            }
-        const bool fire = live && lg > logit_thr;
-        const long long fi = live ? fb.at(aa, bb, kk) : 0;
-        if (live) mask[fi] = fire ? 1 : 0;
-        const unsigned m = __ballot_sync(0xffffffffu, fire);
-        nfire += __popc(m);
-        if (m) {
-            unsigned base = 0;
-            if (lane == 0) base = atomicAdd(count, (unsigned)__popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (fire) {
-                list[base + __popc(m & ((1u << lane) - 1u))] = (unsigned)fi;
-                // the interior cells below (face - 1) and above (face) along DIR: the cell
-                // above has the face's own coordinates
-                const int a = DIR == 0 ? aa : (DIR == 1 ? bb : kk), na = DIR == 0 ? b.nx : (DIR == 1 ? b.ny : b.nz);
-                const long long cell = ((long long)aa * b.ny + bb) * b.nz + kk;
-                const long long step = DIR == 0 ? (long long)b.ny * b.nz : (DIR == 1 ? (long long)b.nz : 1LL);
-                if (a - 1 >= 0) touched[cell - step] = 1;
-                if (a < na) touched[cell] = 1;
-            }
-        }
-    }
-    if (lane == 0 && nfire) atomicAdd(flagged, nfire);
-}
-
-// The same flags on the 5th-generation tensor cores: a CTA of 128 threads takes
+// Flags of every face along DIR on the 5th-generation tensor cores; a flagged
+// face also goes into the compacted list of its axis (FaceBox index) and marks
+// the interior cells on either side as touched, for the correction passes of
+// ns_gate.cu.  A CTA of 128 threads takes
 // 128 faces per tile; their BF16 features (K = 32, the 21 features and zeros)
 // and the network's weight tiles sit in shared memory in the K-major layout, one
 // thread issues two K = 16 tcgen05.mma per layer (M = 128 faces, N = 32 hidden
@@ -1102,15 +944,9 @@ ns_status sensor_step_flags(SensorState* st, const double* U0, const Box& b, con
         const FaceBox& f = fb[d];
         const long long tiles = (long long)((f.n2 + 31) / 32) * ((f.n1 + 3) / 4) * f.n0;
         if (tiles >= (1ll << 31) || f.fstride >= (1ll << 32)) return NS_ERR_UNSUPPORTED;
-#if NS_SENSOR_TCGEN05
         const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 8);
 #define NS_MASK(D) k_sensor_mask_tc<D><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[D], st->flagged, \
                                                           st->list[D], st->counts + D, st->touched, st->err)
-#else
-        const int grid = (int)std::min<long long>(tiles, (long long)st->sms * 6);
-#define NS_MASK(D) k_sensor_mask<D><<<grid, blk, 0, s>>>(st->prim, b, c, f, st->w, thr, st->mask[D], st->flagged, \
-                                                       st->list[D], st->counts + D, st->touched)
-#endif
         if (d == 0) NS_MASK(0);
         else if (d == 1) NS_MASK(1);
         else NS_MASK(2);
