@@ -84,6 +84,7 @@ struct ns_ctx {
     unsigned long long* xslot = nullptr;     // the CFL minimum reduced over the slabs
     bool flags_valid = false;                // the sensor's flags belong to the current state's run
     int sms = 148;                           // multiprocessors of the context's device
+    nsb::WTmaMaps tma[2];                    // FP64 steps: tensor maps of W and W2 (face tiles, viscous planes)
 };
 
 static size_t host_elems(const ns_params* p) {
@@ -263,6 +264,23 @@ static void prof_mark(ns_ctx* ctx, int cls) {
     g_prof->cls[g_prof->n++] = cls;
 }
 
+// TMA-staged FP64 kernels: the y/z faces and the CD-2 viscous terms of the
+// physical semantics (build switches, on by default)
+#ifndef NS_FACE_TMA
+#define NS_FACE_TMA 1
+#endif
+#ifndef NS_VISC_TMA
+#define NS_VISC_TMA 1
+#endif
+
+// the TMA tensor maps of the context's current W (FP64 steps), or null
+static const nsb::WTmaMaps* tma_maps(const ns_ctx* ctx) {
+    if (fp32(ctx)) return nullptr;
+    for (const nsb::WTmaMaps& t : ctx->tma)
+        if (t.ok && t.W == ctx->W) return &t;
+    return nullptr;
+}
+
 // face fluxes of the current (W, U) along every convected axis from first_dir on
 // (U: the context's, or the stage input Uin)
 static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullptr, bool w_only = false) {
@@ -278,9 +296,19 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullp
                 return fail(NS_ERR_CUDA, "gated face kernel launch failed: %s",
                             cudaGetErrorString(cudaGetLastError()));
         } else {
-            launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
-                             phys(ctx), fp32(ctx), ctx->W, U, ctx->box, ctx->c, ctx->F[d],
-                             ctx->fb[d], ctx->stream, w_only);
+            // the TMA tiles serve the physical semantics, whose face stencils read
+            // every cell twice (local LF speed, then the split): from shared memory
+            // that is 7-8% faster than the per-thread kernels on B200, which are 3-7%
+            // faster for the reference semantics' single pass (256^3)
+            const nsb::WTmaMaps* m = (NS_FACE_TMA && w_only && d > 0 && phys(ctx)) ? tma_maps(ctx) : nullptr;
+            if (m)
+                launch_face_flux_tma(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
+                                     phys(ctx), *m, ctx->W, ctx->box, ctx->c, ctx->F[d], ctx->fb[d], ctx->sms,
+                                     ctx->slot + 4, ctx->stream);
+            else
+                launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
+                                 phys(ctx), fp32(ctx), ctx->W, U, ctx->box, ctx->c, ctx->F[d],
+                                 ctx->fb[d], ctx->stream, w_only);
             NS_TRY(check_launch(ctx, d > 0 ? 2 : 1));  // y and z: the face grid and its last plane
         }
         prof_mark(ctx, NS_PROF_FACE_X + d);
@@ -463,8 +491,13 @@ static ns_status do_step(ns_ctx* ctx) {
         if (a.viscous) {  // into the x-face array, which the x-march leaves unused
             a.V = (const double*)ctx->F[0];
             a.vs = ctx->fb[0].fstride;
-            launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
-                           ctx->fb[0].fstride, s);
+            const nsb::WTmaMaps* m = tma_maps(ctx);
+            if (NS_VISC_TMA && m && phys(ctx) && ctx->c.order == 2)
+                launch_viscous_tma(*m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0], ctx->fb[0].fstride,
+                                   ctx->slot + 4, s);
+            else
+                launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
+                               ctx->fb[0].fstride, s);
             NS_TRY(check_launch(ctx, 1));
             prof_mark(ctx, NS_PROF_VISCOUS);
         }
@@ -638,16 +671,21 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
     if (p->convection != NS_CONV_NONE)
         for (int d = 0; d < (p->dim == 3 ? 3 : 2); d++)
             A(&ctx->F[d], (size_t)ctx->fb[d].fstride * NS_NQ * fe);
-    A((void**)&ctx->slot, 4 * sizeof(unsigned long long));
-    // The fused stage kernel serves the FP32 form (both semantics).  In FP64 its
-    // shared-memory ring (one 198 KB block per SM) leaves nothing to overlap the
-    // load and compute phases with, and the FP64-pipe-bound face kernels of the
-    // unfused path run faster (measured on B200 at 256^3: 2.18 vs 3.06 G
-    // cell-updates/s for the characteristic scheme).
+    // [0], [1]: CFL minima by step parity, [2]: scratch minimum, [3]: count of
+    // bad cells (check_finite), [4]: error word of the bounded device waits
+    A((void**)&ctx->slot, 5 * sizeof(unsigned long long));
+    // The fused stage kernel serves the FP32 form (both semantics).  In FP64 the
+    // face kernels + x-march run faster: an FP64 fused stage on an 8 x 16 column
+    // (two 109 KB blocks per SM) measured 1.25-1.56x slower on B200 at 256^3.
     ctx->fused = p->precision == NS_PREC_FP32;
     ctx->xfused = !ctx->fused && p->precision == NS_PREC_FP64 && p->convection != NS_CONV_NONE;
     if (ctx->fused || ctx->xfused) A((void**)&ctx->U2, soa_bytes(ctx->box));
     if (ctx->xfused) A((void**)&ctx->W2, soa_bytes(ctx->box));
+    if (st == NS_OK && ctx->xfused) {
+        // the y/z faces of the FP64 steps read W (and W2, which swaps with it) through TMA tiles
+        nsb::w_tma_encode(&ctx->tma[0], ctx->W, ctx->box);
+        nsb::w_tma_encode(&ctx->tma[1], ctx->W2, ctx->box);
+    }
     A((void**)&ctx->diag, 8 * sizeof(double));
     A((void**)&ctx->clock, 2 * sizeof(double));
     if (st == NS_OK) {
@@ -656,6 +694,7 @@ ns_status ns_create(const ns_params* p, ns_ctx** out) {
         cudaMemsetAsync(ctx->U, 0, soa_bytes(ctx->box), ctx->stream);
         cudaMemsetAsync(ctx->U0, 0, soa_bytes(ctx->box), ctx->stream);
         cudaMemsetAsync(ctx->clock, 0, 2 * sizeof(double), ctx->stream);
+        cudaMemsetAsync(ctx->slot, 0, 5 * sizeof(unsigned long long), ctx->stream);
         if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
             st = fail(NS_ERR_CUDA, "initialisation failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
@@ -823,6 +862,9 @@ ns_status ns_synchronize(ns_ctx* ctx) {
     NS_CUDA(cudaStreamSynchronize(ctx->stream));
     if (ctx->sensor && sensor_status(ctx->sensor) != NS_OK)
         return fail(NS_ERR_TIMEOUT, "a tensor-core wait of the sensor's flag kernel ran out of polls");
+    unsigned long long werr = 0;
+    NS_CUDA(cudaMemcpy(&werr, ctx->slot + 4, sizeof werr, cudaMemcpyDeviceToHost));
+    if (werr) return fail(NS_ERR_TIMEOUT, "a TMA tile wait of a face or viscous kernel ran out of polls");
     return check_state(ctx);
 }
 

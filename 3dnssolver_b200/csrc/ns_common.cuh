@@ -2,9 +2,9 @@
 //
 // Device state layout (HBM): structure of arrays, one plane per variable,
 // each plane the halo'd box (nx+6) x (ny+6) x NZp doubles with k fastest.
-// NZp = nz+6 rounded up to 8 and every plane starts 5 doubles past a 64-byte
-// boundary, so the first interior cell of every k-row (k = 3) is 64-byte
-// aligned and a warp reading 32 consecutive k touches whole 32-byte sectors.
+// NZp = nz+6 rounded up to 8, and the plane stride (fstride) a multiple of 8
+// doubles, so every plane and every k-row starts on a 64-byte boundary (the
+// TMA tensor maps of the FP64 face kernels need 16-byte row strides).
 // Halos are real storage: the boundary fill writes them (the single-GPU form
 // of Domain::apply_boundary_conditions + Communicator::communicate), and the
 // per-operator entry points accept a caller's halos verbatim.
@@ -20,7 +20,7 @@ namespace nsb {
 
 constexpr int NG = 3;
 constexpr int NQV = 5;
-constexpr int PLANE_PAD = 5;  // elements before interior k=3 reaches 64-byte alignment
+constexpr int PLANE_PAD = 5;  // spare elements at the end of every plane
 
 struct Box {
     int nx, ny, nz;     // interior cells

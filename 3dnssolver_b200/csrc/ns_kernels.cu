@@ -4,7 +4,9 @@
 //   k_fill_prim      boundary fill + halo exchange of U on the face halos, then
 //                    W = prim(U) on every cell (time_scheme.cpp:133-135)
 //   k_face_flux<d>   WENO-5 face fluxes along axis d, one thread per face
-//                    (Weno5::x/y/z_sweep, Weno5cw::*_sweep)
+//                    (Weno5::x/y/z_sweep, Weno5cw::*_sweep); the FP64 steps of
+//                    the physical semantics run k_face_flux_tma (ns_tma.cu)
+//                    for y and z and k_viscous_tma for CD-2 viscous terms
 //   k_update         flux differences + centered viscous terms + RK combination
 //                    (Weno5::compute_residual, CenteredDiffusion::compute_residual,
 //                    TimeScheme::substep)
@@ -20,6 +22,8 @@
 #include "ns_eos.cuh"
 #include "ns_face.cuh"
 #include "ns_kernels.h"
+#include "ns_tcgen05.cuh"
+#include "ns_tma.cuh"
 #include "ns_viscous.cuh"
 
 namespace nsb {
@@ -378,34 +382,20 @@ __device__ __forceinline__ void viscous_reference(const double* __restrict__ W, 
 }
 
 // Physical semantics: full 3D viscous stress and heat flux with constant mu
-// (no reference counterpart).  Derivatives along one axis read the
-// boundary-filled W as it is (ghost cells included); a mixed derivative also
-// reads edge and corner cells, which no fill writes, so its offsets are folded
-// back into the interior along each axis (periodic wrap or Neumann clamp; a
-// slab's x ghost planes are the neighbours' cells and stay).  All axis loops
-// unroll at compile time (2D skips the z terms at run time) and the folded
-// offsets are formed once per axis.
-template <int H, typename TV>
-__device__ __forceinline__ void viscous_physical(const double* __restrict__ W, const Box& b,
-                                                 const Consts& c, int i, int j, int k, TV r[5]) {
+// (no reference counterpart), from two accessors of W around the cell:
+// ld1(q, ax, t) = field q at offset t - H along axis ax, ld2(q, a, s, bx, t) =
+// field q at offsets s - H along a and t - H along bx (mixed derivatives).
+// All axis loops unroll at compile time (2D skips the z terms at run time).
+template <int H, typename TV, typename Ld1, typename Ld2>
+__device__ __forceinline__ void viscous_physical_core(Ld1 ld1, Ld2 ld2, const Consts& c, TV r[5]) {
     constexpr int NS = 2 * H + 1;
-    const long long fs = b.fstride;
-    const long long st3[3] = {(long long)b.NY * b.NZp, (long long)b.NZp, 1};
-    const long long o = b.at(i + NG, j + NG, k + NG);
     const bool three = c.dim == 3;
     const double inv[3] = {c.inv_dx, c.inv_dy, c.inv_dz};
-    const int n3[3] = {b.nx, b.ny, b.nz};
-    const int c3[3] = {i, j, k};
-    // offsets of the folded stencil cells along each axis, and the CD coefficients
-    long long off[3][NS];
     TV c1[3][NS], c2[3][NS];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
         for (int t = 0; t < NS; t++) {
-            const int v = c3[a] + t - H;
-            const int f = (a == 0) ? fold_x(v, n3[0], c) : fold(v, n3[a], c.periodic[a]);
-            off[a][t] = (long long)(f - c3[a]) * st3[a];
             c1[a][t] = TV(c.df[3 - H + t] * inv[a]);
             c2[a][t] = TV(c.ddf[3 - H + t] * inv[a] * inv[a]);
         }
@@ -422,11 +412,10 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
         if (bx == 2 && !three) continue;
 #pragma unroll
         for (int t = 0; t < NS; t++) {
-            const long long oo = o + (t - H) * st3[bx];
-            const TV T = TV(W[1 * fs + oo]) / TV(W[oo]);
+            const TV T = TV(ld1(1, bx, t)) / TV(ld1(0, bx, t));
 #pragma unroll
             for (int a = 0; a < 3; a++) {
-                const TV va = TV(W[(2 + a) * fs + oo]);
+                const TV va = TV(ld1(2 + a, bx, t));
                 if (t != H) gu[a][bx] += va * c1[bx][t];
                 lap[a] += va * c2[bx][t];
                 if (a == bx) gdiv[a] += va * c2[bx][t];
@@ -448,14 +437,14 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
 #pragma unroll
                 for (int t = 0; t < NS; t++) {
                     if (t == H) continue;
-                    inner += TV(W[(2 + bx) * fs + o + off[a][s] + off[bx][t]]) * c1[bx][t];
+                    inner += TV(ld2(2 + bx, a, s, bx, t)) * c1[bx][t];
                 }
                 acc += inner * c1[a][s];
             }
             gdiv[a] += acc;
         }
     const TV mu = TV(c.mu), lamb = TV(c.lamb);
-    const TV uv[3] = {TV(W[2 * fs + o]), TV(W[3 * fs + o]), TV(W[4 * fs + o])};
+    const TV uv[3] = {TV(ld1(2, 0, H)), TV(ld1(3, 0, H)), TV(ld1(4, 0, H))};
     const TV div = gu[0][0] + gu[1][1] + gu[2][2];
     TV work = 0, diss = 0, mom[3];
 #pragma unroll
@@ -474,6 +463,35 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
     r[3] -= mom[1];
     r[4] -= mom[2];
     r[1] -= work + diss + TV(c.heat) * mu * lapT;
+}
+
+// The physical viscous terms of cell (i, j, k) read from the device state.
+// Derivatives along one axis read the boundary-filled W as it is (ghost cells
+// included); a mixed derivative also reads edge and corner cells, which no
+// fill writes, so its offsets are folded back into the interior along each
+// axis (periodic wrap or Neumann clamp; a slab's x ghost planes are the
+// neighbours' cells and stay).  The folded offsets are formed once per axis.
+template <int H, typename TV>
+__device__ __forceinline__ void viscous_physical(const double* __restrict__ W, const Box& b,
+                                                 const Consts& c, int i, int j, int k, TV r[5]) {
+    constexpr int NS = 2 * H + 1;
+    const long long fs = b.fstride;
+    const long long st3[3] = {(long long)b.NY * b.NZp, (long long)b.NZp, 1};
+    const long long o = b.at(i + NG, j + NG, k + NG);
+    const int n3[3] = {b.nx, b.ny, b.nz};
+    const int c3[3] = {i, j, k};
+    long long off[3][NS];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int t = 0; t < NS; t++) {
+            const int v = c3[a] + t - H;
+            const int f = (a == 0) ? fold_x(v, n3[0], c) : fold(v, n3[a], c.periodic[a]);
+            off[a][t] = (long long)(f - c3[a]) * st3[a];
+        }
+    auto ld1 = [&](int q, int ax, int t) { return W[q * fs + o + (t - H) * st3[ax]]; };
+    auto ld2 = [&](int q, int a, int s, int bx, int t) { return W[q * fs + o + off[a][s] + off[bx][t]]; };
+    viscous_physical_core<H, TV>(ld1, ld2, c, r);
 }
 
 // ---------------------------------------------------------------------------
@@ -568,13 +586,101 @@ __global__ void __launch_bounds__(128) k_viscous(const double* __restrict__ W, B
     for (int q = 1; q < 5; q++) V[(q - 1) * vs + e] = rv[q];
 }
 
+// Physical semantics, CD-2: the same terms from planes of W that the TMA unit
+// loads into a 4-slot ring while the block marches VISC_LX cells along x.  A
+// block owns 4 rows x 32 columns; one plane is the box z = k0-1 .. k0+32,
+// rows j0-1 .. j0+4 (34 x 6 x 5 fields, halo'd coordinates from k0+2, an even
+// start as TMA requires), so each cell of W crosses L2 once per block instead
+// of once per stencil.  A cell on a domain edge line (at the boundary along
+// two axes or more) needs folded corner cells for its mixed derivatives, which
+// no fill writes and so the box does not hold: it reads the device state like
+// k_viscous.  Waits are bounded (the error word receives 1 and the block ends).
+constexpr int VISC_LX = 32;
+
+__global__ void __launch_bounds__(128, 4)
+    k_viscous_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ W, Box b, Consts c,
+                  double* __restrict__ V, long long vs, unsigned long long* __restrict__ err) {
+    constexpr int BZ = VISC_TMA_BZ, BY = VISC_TMA_BY, QS = BZ * BY, ELEMS = 5 * QS;
+    constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // 128-byte aligned slots
+    constexpr uint32_t BYTES = ELEMS * 8;
+    constexpr int NSLOT = 4;
+    __shared__ __align__(128) double ring[NSLOT * STRIDE];
+    __shared__ __align__(8) unsigned long long full[NSLOT];
+    const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
+    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = blockIdx.z * VISC_LX;
+    const int x1 = min(x0 + VISC_LX, b.nx);
+    const int k = k0 + lane, j = j0 + ty;
+    const bool live = k < b.nz && j < b.ny;
+    // plane p (x0 - 1 <= p <= x1) is the (p - x0 + 1)-th load of the block
+    auto slot = [&](int p) { return (p - x0 + 1) % NSLOT; };
+    auto bar = [&](int p) { return tc::smem_u32(&full[slot(p)]); };
+    auto par = [&](int p) { return (uint32_t)(((p - x0 + 1) / NSLOT) & 1); };
+    auto issue = [&](int p) {
+        mbar_expect_tx(bar(p), BYTES);
+        tma_load_4d(tc::smem_u32(ring + slot(p) * STRIDE), &map, k0 + 2, j0 + 2, p + NG, 0, bar(p));
+    };
+    if (tid == 0)
+        for (int q = 0; q < NSLOT; q++) tc::mbar_init(tc::smem_u32(&full[q]), 1);
+    __syncthreads();
+    const int pre = min(x0 + 2, x1);  // planes in flight before the march
+    if (tid == 0)
+        for (int p = x0 - 1; p <= pre; p++) issue(p);
+    bool ok = tc::mbar_wait(bar(x0 - 1), par(x0 - 1), kTilePolls);
+    ok = ok && tc::mbar_wait(bar(x0), par(x0), kTilePolls);
+    const int nbjk = (j == 0 || j == b.ny - 1) + (k == 0 || k == b.nz - 1);
+    const int cc = (ty + 1) * BZ + lane + 1;
+    int waited = x0;  // planes up to this one have landed
+    for (int i = x0; i < x1; i++) {
+        ok = ok && tc::mbar_wait(bar(i + 1), par(i + 1), kTilePolls);
+        if (ok) waited = i + 1;
+        if (ok && live) {
+            double rv[5] = {0, 0, 0, 0, 0};
+            if (nbjk + (i == 0 || i == b.nx - 1) >= 2) {
+                viscous_physical<1, double>(W, b, c, i, j, k, rv);
+            } else {
+                const double* P[3] = {ring + slot(i - 1) * STRIDE, ring + slot(i) * STRIDE,
+                                      ring + slot(i + 1) * STRIDE};
+                auto at = [&](int q, int ox, int oy, int oz) { return P[1 + ox][q * QS + cc + oy * BZ + oz]; };
+                auto ld1 = [&](int q, int ax, int t) {
+                    const int d = t - 1;
+                    return at(q, ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0);
+                };
+                auto ld2 = [&](int q, int a, int s, int bx, int t) {
+                    int o[3] = {0, 0, 0};
+                    o[a] += s - 1;
+                    o[bx] += t - 1;
+                    return at(q, o[0], o[1], o[2]);
+                };
+                viscous_physical_core<1, double>(ld1, ld2, c, rv);
+            }
+            const long long e = ((long long)i * b.ny + j) * b.nz + k;
+#pragma unroll
+            for (int q = 1; q < 5; q++) V[(q - 1) * vs + e] = rv[q];
+        }
+        // every thread is done with plane i - 1 (and agrees on whether a wait ran out)
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(err, 1ull);
+                // the loads still in flight: planes waited + 1 .. min(i + 2, x1)
+                for (int p = waited + 1; p <= min(i + 2, x1); p++) tc::mbar_wait(bar(p), par(p), kTilePolls);
+            }
+            __syncthreads();
+            return;
+        }
+        if (tid == 0 && i + 3 <= x1) issue(i + 3);  // into the slot of plane i - 1
+    }
+}
+
 // ---------------------------------------------------------------------------
 // FP64 stage, last kernel: x-face fluxes marched along x with the cell update of
 // each cell as soon as both of its x-faces are known (same face and update
 // arithmetic as k_face_flux<0> + k_update).  The x-face array never reaches
 // HBM, and the update's loads (U0, U, the y- and z-face fluxes, W for the
 // viscous terms) overlap the x-faces' FP64 work.  U_out is a second buffer:
-// other threads still read U's x-neighbours for their stencils.
+// other threads still read U's x-neighbours for their stencils.  (A variant that
+// kept each thread's 6-cell W stencil in a shared ring, loading every cell once,
+// ran 5-24% slower on B200 at 256^3, with 70 KB of shared memory per block and
+// three blocks per SM leaving about 30 KB of L1 for everything else.)
 
 // Cells a thread marches: 24 ran 3% faster than 32 at 256^3 (more, shorter
 // blocks balance the SMs better; the extra x-face per block costs less), 20
@@ -910,6 +1016,40 @@ static void face_one(const double* W, const double* U, const Box& b, const Const
         k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb);
 }
 
+template <int DIR, bool CHAR, bool BORGES, bool PHYS>
+static void tail_one(const double* W, const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s) {
+    const dim3 tail(((DIR == 1 ? fb.n2 : fb.n1) + 127) / 128, fb.n0);
+    k_face_flux_tail<DIR, CHAR, BORGES, PHYS, double, double, true><<<tail, 128, 0, s>>>(W, W, b, c, (double*)F, fb);
+}
+
+template <int DIR>
+static void tail_dispatch(bool chr, bool borges, bool phys, const double* W, const Box& b, const Consts& c, void* F,
+                          const FaceBox& fb, cudaStream_t s) {
+    if (chr) {
+        if (borges) {
+            if (phys) tail_one<DIR, true, true, true>(W, b, c, F, fb, s);
+            else tail_one<DIR, true, true, false>(W, b, c, F, fb, s);
+        } else {
+            if (phys) tail_one<DIR, true, false, true>(W, b, c, F, fb, s);
+            else tail_one<DIR, true, false, false>(W, b, c, F, fb, s);
+        }
+    } else {
+        if (borges) {
+            if (phys) tail_one<DIR, false, true, true>(W, b, c, F, fb, s);
+            else tail_one<DIR, false, true, false>(W, b, c, F, fb, s);
+        } else {
+            if (phys) tail_one<DIR, false, false, true>(W, b, c, F, fb, s);
+            else tail_one<DIR, false, false, false>(W, b, c, F, fb, s);
+        }
+    }
+}
+
+void launch_face_tail_w(int dir, bool chr, bool borges, bool phys, const double* W, const Box& b,
+                        const Consts& c, void* F, const FaceBox& fb, cudaStream_t s) {
+    if (dir == 1) tail_dispatch<1>(chr, borges, phys, W, b, c, F, fb, s);
+    else tail_dispatch<2>(chr, borges, phys, W, b, c, F, fb, s);
+}
+
 template <int DIR, typename T, typename TF>
 static void face_dispatch(bool chr, bool borges, bool phys, const double* W, const double* U,
                           const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s,
@@ -997,6 +1137,13 @@ static void xupd_one(const UpdateArgs& a, cudaStream_t s) {
 template <int H, bool PHYS>
 static void visc_one(const double* W, const Box& b, const Consts& c, double* V, long long vs, cudaStream_t s) {
     k_viscous<H, PHYS><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, V, vs);
+}
+
+void launch_viscous_tma(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
+                        long long vs, unsigned long long* err, cudaStream_t s) {
+    const dim3 grid((b.nz + 31) / 32, (b.ny + 3) / 4, (b.nx + VISC_LX - 1) / VISC_LX);
+    k_viscous_tma<<<grid, dim3(32, 4), 0, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[2]), W, b, c, V, vs,
+                                               err);
 }
 
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,

@@ -97,6 +97,28 @@ void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaS
 void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
                       const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
                       cudaStream_t s, bool w_only = false);
+// the last y or z face plane (j = ny or k = nz) of an FP64 time step (W only)
+void launch_face_tail_w(int dir, bool chr, bool borges, bool phys, const double* W, const Box& b,
+                        const Consts& c, void* F, const FaceBox& fb, cudaStream_t s);
+// TMA tensor maps of one W buffer (ns_tma.cu): map[0] the y-face tiles, map[1]
+// the z-face tiles, map[2] the planes of the marched viscous kernel; each
+// holds a CUtensorMap (128 bytes, 64-byte aligned)
+struct WTmaMaps {
+    alignas(64) unsigned char map[3][128];
+    const double* W = nullptr;
+    bool ok = false;
+};
+// box of one plane of the TMA-marched viscous kernel (CD-2): z from kk0 + 2
+// (halo'd, even) 34 wide, rows j0 + 2 .. j0 + 7
+constexpr int VISC_TMA_BZ = 34, VISC_TMA_BY = 6;
+// false (and m->ok false) where TMA cannot serve the buffer: no driver entry
+// point, an unaligned base or too many tiles; the per-thread kernels then run
+bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b);
+// FP64 y- (dir 1) or z-faces (dir 2) of a time step from TMA-loaded tiles of the
+// W that m maps, then the last face plane; *err receives 1 if a wait ran out
+void launch_face_flux_tma(int dir, bool chr, bool borges, bool phys, const WTmaMaps& m, const double* W,
+                          const Box& b, const Consts& c, void* F, const FaceBox& fb, int sms,
+                          unsigned long long* err, cudaStream_t s);
 void launch_update(const UpdateArgs& a, cudaStream_t s);
 // FP64 MODE_STAGE: x-faces + update in one march, U_out = a.Unext (a.F[0] unused)
 void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s);
@@ -104,6 +126,10 @@ void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_
 // vs >= nx ny nz), half-width h = order/2 of the centered scheme
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
                     long long vs, cudaStream_t s);
+// the same for physical semantics and CD-2 from TMA-loaded planes of the W that
+// m maps, marched along x; *err receives 1 if a wait ran out
+void launch_viscous_tma(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
+                        long long vs, unsigned long long* err, cudaStream_t s);
 // slab halo exchange: pack the outer interior planes of a side / unpack into its ghost planes
 void launch_slab_pack(const double* U, const Box& b, int side, double* buf, cudaStream_t s);
 void launch_slab_unpack(double* U, const Box& b, int side, const double* buf, cudaStream_t s);

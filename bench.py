@@ -266,35 +266,50 @@ def job_rate(world, cells, steps, ms_max):
 # ---------------------------------------------------------------------------
 # rooflines
 
-# Floating-point work per unit of each kernel class, counted by ncu on the 128^3
-# shear layer, reference semantics (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}[2]_pred_on.sum
-# divided by the faces or cells of the launch; the counts do not depend on the data):
-# (flop per unit with an FMA as 2, FP lane operations per unit with a packed f32x2
-# operation as 2, pipe, unit).  The fused stage rows are the first two stages.
+# Floating-point work per unit of each kernel class, counted by ncu at 128^3
+# (sm__sass_thread_inst_executed_op_{d,f}{fma,mul,add}[2]_pred_on.sum divided by
+# the faces or cells of the launch; the counts do not depend on the data):
+# (flop per unit with an FMA as 2, FP lane operations per unit with a packed
+# f32x2 operation as 2, pipe, unit), keyed by (semantics, form, kernel class).
+# Reference semantics: the shear layer; physical semantics: the Taylor-Green
+# vortex.  The x-update and fused stage rows average the three stages (the
+# third also forms the next step's start).
 COMPUTE_PER_UNIT = {
-    ("fp64_char", "face_x"): (1325, 953, "fp64", "face"),
-    ("fp64_char", "face_y"): (1325, 953, "fp64", "face"),
-    ("fp64_char", "face_z"): (1318, 946, "fp64", "face"),
-    ("fp64_comp", "face_x"): (965, 729, "fp64", "face"),
-    ("fp64_comp", "face_y"): (965, 729, "fp64", "face"),
-    ("fp64_comp", "face_z"): (941, 705, "fp64", "face"),
-    ("fp64_char", "update"): (316, 205, "fp64", "cell"),
-    ("fp64_comp", "update"): (316, 205, "fp64", "cell"),
-    ("fp64_char", "xface_update"): (1505, 1083, "fp64", "cell"),
-    ("fp64_comp", "xface_update"): (1155, 856, "fp64", "cell"),
-    ("fp64_char", "viscous"): (222, 135, "fp64", "cell"),
-    ("fp64_comp", "viscous"): (222, 135, "fp64", "cell"),
-    ("fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
-    ("fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
+    ("reference", "fp64_char", "face_x"): (1325, 953, "fp64", "face"),
+    ("reference", "fp64_char", "face_y"): (1325, 953, "fp64", "face"),
+    ("reference", "fp64_char", "face_z"): (1318, 946, "fp64", "face"),
+    ("reference", "fp64_comp", "face_x"): (965, 729, "fp64", "face"),
+    ("reference", "fp64_comp", "face_y"): (965, 729, "fp64", "face"),
+    ("reference", "fp64_comp", "face_z"): (941, 705, "fp64", "face"),
+    ("reference", "fp64_char", "update"): (316, 205, "fp64", "cell"),
+    ("reference", "fp64_comp", "update"): (316, 205, "fp64", "cell"),
+    ("reference", "fp64_char", "xface_update"): (1527, 1098, "fp64", "cell"),
+    ("reference", "fp64_comp", "xface_update"): (1155, 856, "fp64", "cell"),
+    ("reference", "fp64_char", "viscous"): (222, 135, "fp64", "cell"),
+    ("reference", "fp64_comp", "viscous"): (222, 135, "fp64", "cell"),
+    ("reference", "fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
+    ("reference", "fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
+    ("physical", "fp64_char", "face_y"): (1441, 1032, "fp64", "face"),
+    ("physical", "fp64_char", "face_z"): (1441, 1032, "fp64", "face"),
+    ("physical", "fp64_char", "xface_update"): (1638, 1166, "fp64", "cell"),
+    ("physical", "fp64_char", "viscous"): (392, 225, "fp64", "cell"),
+    ("physical", "fp32_char", "stage_fused"): (4486, 3070, "fp32", "cell"),
+    ("physical", "fp32_comp", "stage_fused"): (3521, 2448, "fp32", "cell"),
 }
-# DRAM bytes (read + write) per unit from one ncu capture at 128^3 (the kernels
-# stream their inputs once at 128^3 and above, so traffic scales with the units).
+# DRAM bytes (read + write) per unit from ncu captures at 128^3 (inputs larger
+# than L2; the kernels stream their inputs once at 128^3 and above, so traffic
+# scales with the units); stage-averaged like the counts above.
 TRAFFIC_PER_UNIT = {
-    ("fp64_char", "face_x"): 120.4, ("fp64_char", "face_y"): 118.6, ("fp64_char", "face_z"): 113.6,
-    ("fp64_comp", "face_x"): 119.7, ("fp64_comp", "face_y"): 118.7, ("fp64_comp", "face_z"): 113.3,
-    ("fp64_char", "update"): 283.7, ("fp64_comp", "update"): 283.7,
-    ("fp64_char", "xface_update"): 332.7, ("fp64_comp", "xface_update"): 330.3,
-    ("fp64_char", "viscous"): 51.2, ("fp64_comp", "viscous"): 51.2,
+    ("reference", "fp64_char", "face_x"): 120.4, ("reference", "fp64_char", "face_y"): 118.6,
+    ("reference", "fp64_char", "face_z"): 113.6,
+    ("reference", "fp64_comp", "face_x"): 119.7, ("reference", "fp64_comp", "face_y"): 118.7,
+    ("reference", "fp64_comp", "face_z"): 113.3,
+    ("reference", "fp64_char", "update"): 283.7, ("reference", "fp64_comp", "update"): 283.7,
+    ("reference", "fp64_char", "xface_update"): 345.2, ("reference", "fp64_comp", "xface_update"): 343.6,
+    ("reference", "fp64_char", "viscous"): 51.2, ("reference", "fp64_comp", "viscous"): 51.2,
+    ("physical", "fp64_char", "face_y"): 68.4, ("physical", "fp64_char", "face_z"): 65.3,
+    ("physical", "fp64_char", "xface_update"): 329.5, ("physical", "fp64_char", "viscous"): 62.6,
+    ("physical", "fp32_char", "stage_fused"): 118.9, ("physical", "fp32_comp", "stage_fused"): 119.0,
 }
 KERNEL_NAMES = {"stage_fused": "k_stage_march", "update": "k_update", "sensor": "k_sensor_mask",
                 "xface_update": "k_xface_update", "viscous": "k_viscous", "fill_prim": "k_fill_prim/k_fill_halo",
@@ -308,9 +323,11 @@ def profile(s, reps=3):
     return {k: statistics.mean(pr[k] for pr in profs) for k in profs[0]}
 
 
-def rooflines(form, prof, n, ms_per_step, peaks, fma):
+def rooflines(form, prof, n, ms_per_step, peaks, fma, semantics):
     """HBM roofline (algorithmic bytes: 120 B per cell-stage) of the form's dominant
-    kernel class and of the whole step, and the compute roofline of that kernel."""
+    kernel class and of the whole step, and the compute roofline of that kernel
+    (per-unit counts of the workload's semantics)."""
+    sem = "physical" if semantics else "reference"
     cells = n ** 3
     faces = (n + 1) * n * n
     dom = max(prof, key=prof.get)
@@ -320,7 +337,8 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma):
     alg = BYTES_PER_CELL_STAGE * cells  # one stage of every cell per launch
     achieved = alg / (per_launch_ms / 1e3) / 1e9
     units = faces if dom.startswith("face") else cells
-    key = ("fp64_char" if form.startswith("fp64_char") else form.split("_cd6")[0], dom)
+    fkey = "fp64_char" if form.startswith("fp64_char") else form.split("_cd6")[0]
+    key = (sem, fkey, dom)
     tpu = TRAFFIC_PER_UNIT.get(key)
     traffic = round(tpu * units) if tpu else None
     step_alg = 3 * alg
@@ -331,7 +349,7 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma):
     for cls, ms in prof.items():
         if ms <= 0:
             continue
-        t = TRAFFIC_PER_UNIT.get((key[0], cls))
+        t = TRAFFIC_PER_UNIT.get((sem, fkey, cls))
         if t is None:
             covered = False
             continue
@@ -364,7 +382,7 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma):
                 "unit": "TFLOP/s", "frac": round(tflops / peak, 4),
                 "pipe_frac": round(ops_rate / (peak / 2.0), 4),
                 "peak_source": f"measured now: ns_fma_peak ({pipe} FMA chains on every SM)",
-                "counts_source": "ncu per-opcode counts of the reference-semantics kernel at 128^3",
+                "counts_source": f"ncu per-opcode counts of the {sem}-semantics kernel at 128^3",
                 "flop_per_" + unit: flop_u, "fp_ops_per_" + unit: inst_u}
         hbm["note"] = f"{pipe}-pipe bound: see compute_roofline"
     return hbm, comp
@@ -535,7 +553,8 @@ def slab_bench(args, dist, rank, world, local):
     except Exception:
         pass
     fma = {"fp64": pkg.fma_peak(True), "fp32": pkg.fma_peak(False)}
-    roofline, compute_roofline = rooflines(args.form, prof, n, ms / args.steps, peaks, fma)
+    roofline, compute_roofline = rooflines(args.form, prof, n, ms / args.steps, peaks, fma,
+                                           WORKLOADS[wk]["semantics"])
     halo_bytes = 2 * 15 * n * n * 8 * 3  # both sides, 3 planes x 5 fields, 3 stages per step
     if rank == 0:
         out = {
@@ -658,7 +677,8 @@ def main():
     ms_max = rank_max(ms)
     value = job_rate(world, cells, args.steps, ms_max)
     prof = profile(s)
-    roofline, compute_roofline = rooflines(args.form, prof, n, ms_max / args.steps, peaks, fma)
+    roofline, compute_roofline = rooflines(args.form, prof, n, ms_max / args.steps, peaks, fma,
+                                           WORKLOADS[wk]["semantics"])
 
     # end to end through the C ABI with host buffers: ns_time_step uploads W from pinned
     # host memory, runs the step and downloads W every step
@@ -689,7 +709,7 @@ def main():
             s2, ms2, l2, _ = time_form(f, args.steps, args.warmup)
             ms2 = rank_max(ms2)
             pr2 = profile(s2)
-            hbm2, comp2 = rooflines(f, pr2, n, ms2 / args.steps, peaks, fma)
+            hbm2, comp2 = rooflines(f, pr2, n, ms2 / args.steps, peaks, fma, WORKLOADS[wk]["semantics"])
             s2.close()
             forms[f] = {"value": job_rate(world, cells, args.steps, ms2), "ms_per_step": ms2 / args.steps,
                         "gpu_launches": l2, "vs_" + args.form: ms_max / ms2,

@@ -224,8 +224,20 @@ def test_physical_semantics_rhs_matches_oracle(oracle, shape, conv, order, bc, d
     assert ok.all(), f"rel L2 per field {err}"
 
 
-def test_physical_semantics_steps_match_oracle(oracle):
-    p = pkg.make_params(14, 12, 10, convection=2, diffusion_order=4, bc=(N, P, P), mu=0.02, cfl=0.4,
+# the FP64 physical steps run the TMA-staged y/z face kernels and, with CD-2, the
+# TMA-marched viscous kernel: odd and partial tiles, domain edge lines (Neumann
+# and periodic), several x-blocks of the viscous march, 2D
+PHYS_STEP_CASES = [
+    ((14, 12, 10), 3, 2, 4, (N, P, P)),
+    ((19, 13, 35), 3, 2, 2, (N, N, N)),
+    ((70, 6, 33), 3, 1, 2, (P, N, P)),
+    ((21, 9, 1), 2, 2, 2, (N, P, P)),
+]
+
+
+@pytest.mark.parametrize("shape,dim,conv,order,bc", PHYS_STEP_CASES)
+def test_physical_semantics_steps_match_oracle(oracle, shape, dim, conv, order, bc):
+    p = pkg.make_params(*shape, dim=dim, convection=conv, diffusion_order=order, bc=bc, mu=0.02, cfl=0.4,
                         semantics=pkg.SEM_PHYSICAL)
     W0 = wl.random_field(p, seed=19, smooth=False)
     Wo, Uo, dto = oracle.run(p, W0, 3)

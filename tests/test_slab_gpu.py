@@ -58,6 +58,8 @@ CASES = [
     ((24, 10, 12), 2, (P, P, P), 2, 2, pkg.PREC_FP64, pkg.SEM_REFERENCE),
     ((27, 8, 10), 3, (N, P, N), 2, 4, pkg.PREC_FP64, pkg.SEM_REFERENCE),
     ((20, 12, 8), 2, (N, N, P), 1, 6, pkg.PREC_FP64, pkg.SEM_PHYSICAL),
+    # the TMA-staged y/z faces and CD-2 viscous march on slabs with exchanged and Neumann x ends
+    ((26, 9, 35), 2, (N, N, P), 2, 2, pkg.PREC_FP64, pkg.SEM_PHYSICAL),
     ((40, 10, 12), 2, (P, P, N), 2, 2, pkg.PREC_FP32, pkg.SEM_REFERENCE),
     ((33, 9, 8), 3, (N, P, P), 2, 4, pkg.PREC_FP32, pkg.SEM_PHYSICAL),
     ((24, 8, 8), 2, (P, P, P), pkg.CONV_NONE, 2, pkg.PREC_FP64, pkg.SEM_REFERENCE),
