@@ -174,10 +174,14 @@ NS_API ns_status ns_advance(ns_ctx* ctx, int nsteps);
  * first step): TimeScheme::get_dt (src/time_scheme.hpp:31) plus the Driver's
  * time accumulation (src/driver.cpp:54-58).  Waits for the context's stream. */
 NS_API ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time);
-/* Blocks until the context's stream is idle.  With params.check_finite set it
- * then checks the current state: NS_ERR_NONFINITE if an interior cell holds
- * NaN/Inf or a non-positive density or pressure (the message gives the number
- * of such cells).  ns_time_step runs the same check after its step. */
+/* Blocks until the context's stream is idle.  NS_ERR_TIMEOUT if a bounded
+ * device wait ran out since the context was created (a tensor-core wait of the
+ * sensor's flag kernel, or a TMA tile wait of the FP64 face or viscous
+ * kernels; the kernel then ended without its results).  With
+ * params.check_finite set it then checks the current state: NS_ERR_NONFINITE if
+ * an interior cell holds NaN/Inf or a non-positive density or pressure (the
+ * message gives the number of such cells).  ns_time_step runs the same check
+ * after its step. */
 NS_API ns_status ns_synchronize(ns_ctx* ctx);
 NS_API ns_status ns_get_diagnostics(ns_ctx* ctx, ns_diagnostics* out);
 /* Kernel classes timed by ns_profile_step (NS_PROF_SENSOR: the per-step
