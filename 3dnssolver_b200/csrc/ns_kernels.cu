@@ -695,8 +695,15 @@ __global__ void __launch_bounds__(128, 4)
 // stage result, as the reference's U holds it between steps.  In the first stage U
 // and U0 are one buffer, only read; U0 is written in the third stage only, where
 // it is not U (so the restrict qualifiers hold).
+// Resident blocks per SM requested for the characteristic-wise march: the
+// reference semantics' march ran 7% faster at 2 (255 registers, no spills) than
+// at 3 (168 registers, spills), the physical semantics' 13% slower (B200, 256^3).
+template <bool CHAR, bool PHYS>
+struct XupdMinBlocks {
+    static constexpr int value = CHAR ? (PHYS ? 3 : 2) : FaceMinBlocks<false, double>::value;
+};
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
-__global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, double>::value)
+__global__ void __launch_bounds__(128, XupdMinBlocks<CHAR, PHYS>::value)
     k_xface_update(const double* __restrict__ W, const double* __restrict__ U, double* __restrict__ U0,
                    double* __restrict__ Uout, double* __restrict__ Wn,
                    const double* __restrict__ Fy, const double* __restrict__ Fz,

@@ -275,43 +275,47 @@ def job_rate(world, cells, steps, ms_max):
 # vortex.  The x-update and fused stage rows average the three stages (the
 # third also forms the next step's start).
 COMPUTE_PER_UNIT = {
-    ("reference", "fp64_char", "face_x"): (1325, 953, "fp64", "face"),
-    ("reference", "fp64_char", "face_y"): (1325, 953, "fp64", "face"),
-    ("reference", "fp64_char", "face_z"): (1318, 946, "fp64", "face"),
-    ("reference", "fp64_comp", "face_x"): (965, 729, "fp64", "face"),
-    ("reference", "fp64_comp", "face_y"): (965, 729, "fp64", "face"),
-    ("reference", "fp64_comp", "face_z"): (941, 705, "fp64", "face"),
-    ("reference", "fp64_char", "update"): (316, 205, "fp64", "cell"),
-    ("reference", "fp64_comp", "update"): (316, 205, "fp64", "cell"),
-    ("reference", "fp64_char", "xface_update"): (1527, 1098, "fp64", "cell"),
-    ("reference", "fp64_comp", "xface_update"): (1155, 856, "fp64", "cell"),
-    ("reference", "fp64_char", "viscous"): (222, 135, "fp64", "cell"),
-    ("reference", "fp64_comp", "viscous"): (222, 135, "fp64", "cell"),
-    ("reference", "fp32_char", "stage_fused"): (4137, 2831, "fp32", "cell"),
-    ("reference", "fp32_comp", "stage_fused"): (3177, 2218, "fp32", "cell"),
+    ("reference", "fp64_char", "face_y"): (1395, 1003, "fp64", "face"),
+    ("reference", "fp64_char", "face_z"): (1395, 1003, "fp64", "face"),
+    ("reference", "fp64_comp", "face_y"): (1041, 789, "fp64", "face"),
+    ("reference", "fp64_comp", "face_z"): (1041, 789, "fp64", "face"),
+    ("reference", "fp64_char", "xface_update"): (1527, 1097, "fp64", "cell"),
+    ("reference", "fp64_comp", "xface_update"): (1178, 872, "fp64", "cell"),
+    ("reference", "fp64_char", "viscous"): (222, 136, "fp64", "cell"),
+    ("reference", "fp64_comp", "viscous"): (222, 136, "fp64", "cell"),
+    ("reference", "fp32_char", "stage_fused"): (4216, 2885, "fp32", "cell"),
+    ("reference", "fp32_comp", "stage_fused"): (3211, 2244, "fp32", "cell"),
     ("physical", "fp64_char", "face_y"): (1441, 1032, "fp64", "face"),
     ("physical", "fp64_char", "face_z"): (1441, 1032, "fp64", "face"),
+    ("physical", "fp64_comp", "face_y"): (1078, 802, "fp64", "face"),
+    ("physical", "fp64_comp", "face_z"): (1078, 802, "fp64", "face"),
     ("physical", "fp64_char", "xface_update"): (1638, 1166, "fp64", "cell"),
-    ("physical", "fp64_char", "viscous"): (392, 225, "fp64", "cell"),
+    ("physical", "fp64_comp", "xface_update"): (1255, 923, "fp64", "cell"),
+    ("physical", "fp64_char", "viscous"): (369, 202, "fp64", "cell"),
+    ("physical", "fp64_comp", "viscous"): (369, 202, "fp64", "cell"),
     ("physical", "fp32_char", "stage_fused"): (4486, 3070, "fp32", "cell"),
     ("physical", "fp32_comp", "stage_fused"): (3521, 2448, "fp32", "cell"),
 }
-# DRAM bytes (read + write) per unit from ncu captures at 128^3 (inputs larger
-# than L2; the kernels stream their inputs once at 128^3 and above, so traffic
-# scales with the units); stage-averaged like the counts above.
+# DRAM bytes (read + write) per unit from the same captures at 128^3 (inputs
+# larger than L2; the kernels stream their inputs once at 128^3 and above, so
+# traffic scales with the units), averaged over the three stages of a step
+# like the counts above; "fill" is the steady-state k_fill_halo.
 TRAFFIC_PER_UNIT = {
-    ("reference", "fp64_char", "face_x"): 120.4, ("reference", "fp64_char", "face_y"): 118.6,
-    ("reference", "fp64_char", "face_z"): 113.6,
-    ("reference", "fp64_comp", "face_x"): 119.7, ("reference", "fp64_comp", "face_y"): 118.7,
-    ("reference", "fp64_comp", "face_z"): 113.3,
-    ("reference", "fp64_char", "update"): 283.7, ("reference", "fp64_comp", "update"): 283.7,
-    ("reference", "fp64_char", "xface_update"): 345.2, ("reference", "fp64_comp", "xface_update"): 343.6,
+    ("reference", "fp64_char", "face_y"): 68.6, ("reference", "fp64_char", "face_z"): 65.7,
+    ("reference", "fp64_comp", "face_y"): 66.0, ("reference", "fp64_comp", "face_z"): 63.2,
+    ("reference", "fp64_char", "xface_update"): 330.2, ("reference", "fp64_comp", "xface_update"): 327.8,
     ("reference", "fp64_char", "viscous"): 51.2, ("reference", "fp64_comp", "viscous"): 51.2,
-    ("physical", "fp64_char", "face_y"): 68.4, ("physical", "fp64_char", "face_z"): 65.3,
-    ("physical", "fp64_char", "xface_update"): 329.5, ("physical", "fp64_char", "viscous"): 62.6,
+    ("reference", "fp64_char", "fill_prim"): 21.8, ("reference", "fp64_comp", "fill_prim"): 21.7,
+    ("reference", "fp32_char", "stage_fused"): 119.2, ("reference", "fp32_comp", "stage_fused"): 119.4,
+    ("physical", "fp64_char", "face_y"): 67.3, ("physical", "fp64_char", "face_z"): 65.3,
+    ("physical", "fp64_comp", "face_y"): 65.1, ("physical", "fp64_comp", "face_z"): 62.5,
+    ("physical", "fp64_char", "xface_update"): 329.5, ("physical", "fp64_comp", "xface_update"): 328.9,
+    ("physical", "fp64_char", "viscous"): 61.6, ("physical", "fp64_comp", "viscous"): 61.7,
+    ("physical", "fp64_char", "fill_prim"): 21.6, ("physical", "fp64_comp", "fill_prim"): 21.9,
     ("physical", "fp32_char", "stage_fused"): 118.9, ("physical", "fp32_comp", "stage_fused"): 119.0,
 }
-KERNEL_NAMES = {"stage_fused": "k_stage_march", "update": "k_update", "sensor": "k_sensor_mask",
+KERNEL_NAMES = {"stage_fused": "k_stage_march", "update": "k_update",
+                "sensor": "k_sensor_prims + k_sensor_mask_tc + k_gate_delta/k_gate_apply",
                 "xface_update": "k_xface_update", "viscous": "k_viscous", "fill_prim": "k_fill_prim/k_fill_halo",
                 "step_begin": "k_step_begin", "face_x": "k_face_flux<x>", "face_y": "k_face_flux<y>",
                 "face_z": "k_face_flux<z>"}
@@ -354,7 +358,12 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma, semantics):
             covered = False
             continue
         step_traffic += t * (faces if cls.startswith("face") else cells) * (1 if cls == "step_begin" else 3)
-    kname = KERNEL_NAMES.get(dom, dom) + f" ({form})"
+    kname = KERNEL_NAMES.get(dom, dom)
+    if sem == "physical" and dom in ("face_y", "face_z"):
+        kname = kname.replace("k_face_flux", "k_face_flux_tma")
+    if sem == "physical" and dom == "viscous" and FORMS[form].get("order", 2) == 2:
+        kname = "k_viscous_tma"
+    kname += f" ({form})"
     hbm = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
            "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
            "traffic_over_algorithmic": round(traffic / alg, 3) if traffic else None,
