@@ -381,8 +381,10 @@ __device__ __forceinline__ void viscous_reference(const double* __restrict__ W, 
                                 TV(W[1 * fs + o]), TV(W[o]), c, r);
 }
 
-// Physical semantics: full 3D viscous stress and heat flux with constant mu
-// (no reference counterpart), from two accessors of W around the cell:
+// Physical semantics: the full 3D viscous terms of viscous_physical below, in
+// the same arithmetic order, from two accessors of W around the cell (the
+// TMA-marched kernel reads its shared-memory planes through them; the
+// per-thread kernel keeps its own loads, which compile to fewer registers):
 // ld1(q, ax, t) = field q at offset t - H along axis ax, ld2(q, a, s, bx, t) =
 // field q at offsets s - H along a and t - H along bx (mixed derivatives).
 // All axis loops unroll at compile time (2D skips the z terms at run time).
@@ -465,12 +467,14 @@ __device__ __forceinline__ void viscous_physical_core(Ld1 ld1, Ld2 ld2, const Co
     r[1] -= work + diss + TV(c.heat) * mu * lapT;
 }
 
-// The physical viscous terms of cell (i, j, k) read from the device state.
-// Derivatives along one axis read the boundary-filled W as it is (ghost cells
-// included); a mixed derivative also reads edge and corner cells, which no
-// fill writes, so its offsets are folded back into the interior along each
-// axis (periodic wrap or Neumann clamp; a slab's x ghost planes are the
-// neighbours' cells and stay).  The folded offsets are formed once per axis.
+// Physical semantics: full 3D viscous stress and heat flux with constant mu
+// (no reference counterpart).  Derivatives along one axis read the
+// boundary-filled W as it is (ghost cells included); a mixed derivative also
+// reads edge and corner cells, which no fill writes, so its offsets are folded
+// back into the interior along each axis (periodic wrap or Neumann clamp; a
+// slab's x ghost planes are the neighbours' cells and stay).  All axis loops
+// unroll at compile time (2D skips the z terms at run time) and the folded
+// offsets are formed once per axis.
 template <int H, typename TV>
 __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, const Box& b,
                                                  const Consts& c, int i, int j, int k, TV r[5]) {
@@ -478,9 +482,13 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
     const long long fs = b.fstride;
     const long long st3[3] = {(long long)b.NY * b.NZp, (long long)b.NZp, 1};
     const long long o = b.at(i + NG, j + NG, k + NG);
+    const bool three = c.dim == 3;
+    const double inv[3] = {c.inv_dx, c.inv_dy, c.inv_dz};
     const int n3[3] = {b.nx, b.ny, b.nz};
     const int c3[3] = {i, j, k};
+    // offsets of the folded stencil cells along each axis, and the CD coefficients
     long long off[3][NS];
+    TV c1[3][NS], c2[3][NS];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
@@ -488,10 +496,74 @@ __device__ __forceinline__ void viscous_physical(const double* __restrict__ W, c
             const int v = c3[a] + t - H;
             const int f = (a == 0) ? fold_x(v, n3[0], c) : fold(v, n3[a], c.periodic[a]);
             off[a][t] = (long long)(f - c3[a]) * st3[a];
+            c1[a][t] = TV(c.df[3 - H + t] * inv[a]);
+            c2[a][t] = TV(c.ddf[3 - H + t] * inv[a] * inv[a]);
         }
-    auto ld1 = [&](int q, int ax, int t) { return W[q * fs + o + (t - H) * st3[ax]]; };
-    auto ld2 = [&](int q, int a, int s, int bx, int t) { return W[q * fs + o + off[a][s] + off[bx][t]]; };
-    viscous_physical_core<H, TV>(ld1, ld2, c, r);
+    TV gu[3][3], lap[3], gdiv[3], lapT = 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        lap[a] = 0;
+        gdiv[a] = 0;
+#pragma unroll
+        for (int bx = 0; bx < 3; bx++) gu[a][bx] = 0;
+    }
+#pragma unroll
+    for (int bx = 0; bx < 3; bx++) {
+        if (bx == 2 && !three) continue;
+#pragma unroll
+        for (int t = 0; t < NS; t++) {
+            const long long oo = o + (t - H) * st3[bx];
+            const TV T = TV(W[1 * fs + oo]) / TV(W[oo]);
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const TV va = TV(W[(2 + a) * fs + oo]);
+                if (t != H) gu[a][bx] += va * c1[bx][t];
+                lap[a] += va * c2[bx][t];
+                if (a == bx) gdiv[a] += va * c2[bx][t];
+            }
+            lapT += T * c2[bx][t];
+        }
+    }
+    // grad(div u)_a += d/dx_a (d u_b / dx_b) for b != a
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int bx = 0; bx < 3; bx++) {
+            if (a == bx || ((a == 2 || bx == 2) && !three)) continue;
+            TV acc = 0;
+#pragma unroll
+            for (int s = 0; s < NS; s++) {
+                if (s == H) continue;
+                TV inner = 0;
+#pragma unroll
+                for (int t = 0; t < NS; t++) {
+                    if (t == H) continue;
+                    inner += TV(W[(2 + bx) * fs + o + off[a][s] + off[bx][t]]) * c1[bx][t];
+                }
+                acc += inner * c1[a][s];
+            }
+            gdiv[a] += acc;
+        }
+    const TV mu = TV(c.mu), lamb = TV(c.lamb);
+    const TV uv[3] = {TV(W[2 * fs + o]), TV(W[3 * fs + o]), TV(W[4 * fs + o])};
+    const TV div = gu[0][0] + gu[1][1] + gu[2][2];
+    TV work = 0, diss = 0, mom[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        mom[a] = mu * lap[a] + (mu + lamb) * gdiv[a];
+        work += uv[a] * mom[a];
+    }
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int bx = 0; bx < 3; bx++) {
+            const TV tab = mu * (gu[a][bx] + gu[bx][a]) + (a == bx ? lamb * div : TV(0));
+            diss += tab * gu[a][bx];
+        }
+    r[2] -= mom[0];
+    r[3] -= mom[1];
+    r[4] -= mom[2];
+    r[1] -= work + diss + TV(c.heat) * mu * lapT;
 }
 
 // ---------------------------------------------------------------------------
