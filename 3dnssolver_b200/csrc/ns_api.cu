@@ -272,6 +272,9 @@ static void prof_mark(ns_ctx* ctx, int cls) {
 #ifndef NS_VISC_TMA
 #define NS_VISC_TMA 1
 #endif
+#ifndef NS_XUPD_TMA
+#define NS_XUPD_TMA 1
+#endif
 
 // the TMA tensor maps of the context's current W (FP64 steps), or null
 static const nsb::WTmaMaps* tma_maps(const ns_ctx* ctx) {
@@ -510,7 +513,12 @@ static ns_status do_step(ns_ctx* ctx) {
         a.m2 = m2[st];
         a.mc = mc[st];
         a.clock = (st == 0) ? ctx->clock : nullptr;
-        launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
+        const nsb::WTmaMaps* xm = NS_XUPD_TMA ? tma_maps(ctx) : nullptr;
+        if (xm)
+            launch_xface_update_tma(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a,
+                                    *xm, ctx->slot + 4, s);
+        else
+            launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
         NS_TRY(check_launch(ctx, 1));
         std::swap(ctx->W, ctx->W2);
         prof_mark(ctx, NS_PROF_XFACE_UPDATE);

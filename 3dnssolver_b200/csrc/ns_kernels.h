@@ -101,10 +101,10 @@ void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, cons
 void launch_face_tail_w(int dir, bool chr, bool borges, bool phys, const double* W, const Box& b,
                         const Consts& c, void* F, const FaceBox& fb, cudaStream_t s);
 // TMA tensor maps of one W buffer (ns_tma.cu): map[0] the y-face tiles, map[1]
-// the z-face tiles, map[2] the planes of the marched viscous kernel; each
-// holds a CUtensorMap (128 bytes, 64-byte aligned)
+// the z-face tiles, map[2] the planes of the marched viscous kernel, map[3] the
+// x-march's planes; each holds a CUtensorMap (128 bytes, 64-byte aligned)
 struct WTmaMaps {
-    alignas(64) unsigned char map[3][128];
+    alignas(64) unsigned char map[4][128];
     const double* W = nullptr;
     bool ok = false;
 };
@@ -122,6 +122,10 @@ void launch_face_flux_tma(int dir, bool chr, bool borges, bool phys, const WTmaM
 void launch_update(const UpdateArgs& a, cudaStream_t s);
 // FP64 MODE_STAGE: x-faces + update in one march, U_out = a.Unext (a.F[0] unused)
 void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s);
+// the same with the x-stencil's W from TMA-loaded planes of the W that m maps
+// (a.W is that W); *err receives 1 if a wait ran out
+void launch_xface_update_tma(bool chr, bool borges, const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err,
+                             cudaStream_t s);
 // viscous terms (components 1..4) of every interior cell into V (plane stride
 // vs >= nx ny nz), half-width h = order/2 of the centered scheme
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,

@@ -142,6 +142,170 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
 }
 
 // ---------------------------------------------------------------------------
+// The FP64 stage's x-march (k_xface_update's work) with its W stencil from a
+// ring of 7 TMA-loaded planes: a block owns 4 rows x 32 columns and marches
+// XT_LX cells along x; plane p's tile (z from k0+2, 34 wide, rows j0..j0+3,
+// 5 fields; 5.4 KB) lands on its own mbarrier.  Planes i-2 .. i+3 feed the
+// x-face between cells i and i+1 while plane i+4 is in flight; after the face
+// the block's threads release plane i-2 together (one block barrier) and
+// plane i+5 takes its slot.  The cell update's operands (U0, U, the y- and
+// z-face fluxes, the viscous terms) still come per thread with cp.async, and
+// the update itself is k_xface_update's.  Two blocks per SM, so the
+// characteristic-wise face keeps its registers without spilling.
+constexpr int XT_LX = 32;
+
+template <int H>
+struct XTmaLayout {
+    static constexpr int BZ = 34, BY = 4, QS = BZ * BY, ELEMS = 5 * QS;
+    static constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // doubles per slot, 128-byte aligned
+    static constexpr int NSLOT = 7;
+    static constexpr int NOP = H > 0 ? 34 : 30;
+    static constexpr uint32_t TX = ELEMS * 8;
+    static constexpr size_t bytes = (size_t)(NSLOT * STRIDE + (5 + NOP) * 128) * 8 + NSLOT * 8;
+};
+
+template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
+__global__ void __launch_bounds__(128, 2)
+    k_xface_update_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ U, double* __restrict__ U0,
+                       double* __restrict__ Uout, double* __restrict__ Wn, const double* __restrict__ Fy,
+                       const double* __restrict__ Fz, const double* __restrict__ V, long long vs, Box b, FaceBox fy,
+                       FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
+                       unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
+                       double* __restrict__ clock, unsigned long long* __restrict__ err) {
+    using XL = XTmaLayout<H>;
+    extern __shared__ __align__(128) unsigned char xsm[];
+    double* ring = reinterpret_cast<double*>(xsm);  // [NSLOT][5][BY][BZ]
+    double* fprev = ring + XL::NSLOT * XL::STRIDE;   // [5][128]
+    double* opnd = fprev + 5 * 128;                  // [NOP][128]
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(opnd + XL::NOP * 128);
+    const int lane = threadIdx.x, ty = threadIdx.y, t = ty * 32 + lane;
+    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = blockIdx.z * XT_LX;
+    const int k = k0 + lane, j = j0 + ty;
+    const int x1 = min(x0 + XT_LX, b.nx);
+    const bool live = k < b.nz && j < b.ny;
+    double best = INFINITY;
+    const double dt = fmin(1e10, __longlong_as_double((long long)*slot)) * c.cfl;
+    const double m3 = mc * dt;
+    if (clock && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0) {
+        clock[0] = dt;
+        clock[1] += dt;
+    }
+    // plane p (x0 - 3 <= p <= x1 + 2) is the (p - x0 + 3)-th load of the block
+    auto sl = [&](int p) { return (p - x0 + 3) % XL::NSLOT; };
+    auto bar = [&](int p) { return tc::smem_u32(&full[sl(p)]); };
+    auto par = [&](int p) { return (uint32_t)(((p - x0 + 3) / XL::NSLOT) & 1); };
+    auto issue = [&](int p) {
+        mbar_expect_tx(bar(p), XL::TX);
+        tma_load_4d(tc::smem_u32(ring + sl(p) * XL::STRIDE), &map, k0 + 2, j0 + NG, p + NG, 0, bar(p));
+    };
+    if (t == 0)
+        for (int q = 0; q < XL::NSLOT; q++) tc::mbar_init(tc::smem_u32(&full[q]), 1);
+    __syncthreads();
+    const int last = x1 + 2;  // the last plane any x-face of the block reads
+    if (t == 0)
+        for (int p = x0 - 3; p <= min(x0 + 3, last); p++) issue(p);
+    bool ok = true;
+    for (int p = x0 - 3; p <= x0 + 2; p++) ok = ok && tc::mbar_wait(bar(p), par(p), kTilePolls);
+    int waited = ok ? x0 + 2 : x0 - 4;
+    const int cc = ty * XL::BZ + lane + 1;
+    // x-face a (between cells a-1 and a) of this thread's column: cells a-3 .. a+2
+    auto xface = [&](int a, double out[5]) {
+        auto ld = [&](int st, double w[5], double u[5]) {
+            const double* P = ring + sl(a - 3 + st) * XL::STRIDE + cc;
+#pragma unroll
+            for (int q = 0; q < 5; q++) w[q] = P[q * XL::QS];
+            cons_from_prim(w, c.inv_gm1, u);
+        };
+        double fL[5][5], fR[5][5], wa[5];
+        face_stencil_from<0, CHAR, PHYS, double>(ld, c, fL, fR, wa);
+        if constexpr (!CHAR)
+            face_comp<double, BORGES>(fL, fR, out);
+        else
+            face_char<0, PHYS, double, BORGES>(fL, fR, wa, c.gamma, c.inv_gm1, out);
+    };
+    const bool convz = flags & UPD_CONVZ;
+    for (int i = x0 - 1; i < x1; i++) {
+        const long long o = b.at(i + NG, j + NG, k + NG);
+        if (i >= x0 && live) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                cp_async8(&opnd[q * 128 + t], U0 + q * b.fstride + o);
+                cp_async8(&opnd[(5 + q) * 128 + t], U + q * b.fstride + o);
+                cp_async8(&opnd[(10 + q) * 128 + t], Fy + q * fy.fstride + fy.at(i, j, k));
+                cp_async8(&opnd[(15 + q) * 128 + t], Fy + q * fy.fstride + fy.at(i, j + 1, k));
+                if (convz) {
+                    cp_async8(&opnd[(20 + q) * 128 + t], Fz + q * fz.fstride + fz.at(i, j, k));
+                    cp_async8(&opnd[(25 + q) * 128 + t], Fz + q * fz.fstride + fz.at(i, j, k + 1));
+                }
+            }
+            if constexpr (H > 0) {
+                const long long e = ((long long)i * b.ny + j) * b.nz + k;
+#pragma unroll
+                for (int q = 0; q < 4; q++) cp_async8(&opnd[(30 + q) * 128 + t], V + q * vs + e);
+            }
+        }
+        cp_async_commit();
+        if (ok && i + 3 > waited) {
+            ok = tc::mbar_wait(bar(i + 3), par(i + 3), kTilePolls);
+            if (ok) waited = i + 3;
+        }
+        double f[5] = {0, 0, 0, 0, 0};
+        if (ok && live) xface(i + 1, f);
+        // every thread is done with plane i - 2 (and agrees on whether a wait ran out)
+        if (__syncthreads_or(!ok)) {
+            cp_async_wait_all();
+            if (t == 0) {
+                atomicOr(err, 1ull);
+                // the loads still in flight: planes waited + 1 .. min(i + 4, last)
+                for (int p = waited + 1; p <= min(i + 4, last); p++) tc::mbar_wait(bar(p), par(p), kTilePolls);
+            }
+            __syncthreads();
+            return;
+        }
+        if (t == 0 && i + 5 <= last) issue(i + 5);  // into the slot of plane i - 2
+        if (i < x0) {
+#pragma unroll
+            for (int q = 0; q < 5; q++) fprev[q * 128 + t] = f[q];
+            continue;
+        }
+        cp_async_wait_all();
+        if (!live) continue;
+        // residual in k_update's order: x, y, z differences, then the viscous terms
+        double r[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            r[q] += (f[q] - fprev[q * 128 + t]) * c.inv_dx;
+            fprev[q * 128 + t] = f[q];
+            r[q] += (opnd[(15 + q) * 128 + t] - opnd[(10 + q) * 128 + t]) * c.inv_dy;
+            if (convz) r[q] += (opnd[(25 + q) * 128 + t] - opnd[(20 + q) * 128 + t]) * c.inv_dz;
+        }
+        if constexpr (H > 0) {
+#pragma unroll
+            for (int q = 1; q < 5; q++) r[q] += opnd[(29 + q) * 128 + t];
+        }
+        double un[5], w[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            un[q] = (opnd[q * 128 + t] * m1) + (opnd[(5 + q) * 128 + t] * m2) + (r[q] * m3);
+            Uout[q * b.fstride + o] = un[q];
+        }
+        prim_from_cons(un, c.gm1, w);  // the next stage's W
+        if constexpr (LAST) {
+            double u0[5];
+            const double d = PHYS ? local_dt_physical(w, c) : local_dt(w, c);
+            if (d < best) best = d;  // NaN never lowers the minimum
+            cons_from_prim(w, c.inv_gm1, u0);
+#pragma unroll
+            for (int q = 0; q < 5; q++) U0[q * b.fstride + o] = u0[q];
+            prim_from_cons(u0, c.gm1, w);  // the next step's first stage reads prim(U0)
+        }
+#pragma unroll
+        for (int q = 0; q < 5; q++) Wn[q * b.fstride + o] = w[q];
+    }
+    if constexpr (LAST) block_min_to(best, slot_next);
+}
+
+// ---------------------------------------------------------------------------
 // host side
 
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -170,8 +334,9 @@ bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b) {
     const cuuint32_t box1[4] = {FaceTile<1>::BZ, FaceTile<1>::BY, 1, 5};
     const cuuint32_t box2[4] = {FaceTile<2>::BZ, FaceTile<2>::BY, 1, 5};
     const cuuint32_t boxv[4] = {VISC_TMA_BZ, VISC_TMA_BY, 1, 5};
-    const cuuint32_t* boxes[3] = {box1, box2, boxv};
-    for (int d = 0; d < 3; d++) {
+    const cuuint32_t boxx[4] = {XTmaLayout<0>::BZ, XTmaLayout<0>::BY, 1, 5};
+    const cuuint32_t* boxes[4] = {box1, box2, boxv, boxx};
+    for (int d = 0; d < 4; d++) {
         CUresult r = enc(reinterpret_cast<CUtensorMap*>(m->map[d]), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
                          const_cast<double*>(W), dims, strides, boxes[d], estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -211,6 +376,42 @@ static void tma_dispatch(bool chr, bool borges, bool phys, const WTmaMaps& m, co
             if (phys) tma_one<DIR, false, false, true>(m, b, c, F, fb, sms, err, s);
             else tma_one<DIR, false, false, false>(m, b, c, F, fb, sms, err, s);
         }
+    }
+}
+
+template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
+static void xt_launch(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s) {
+    constexpr size_t bytes = XTmaLayout<H>::bytes;
+    auto kern = k_xface_update_tma<CHAR, BORGES, PHYS, H, LAST>;
+    // the attribute is per device; a refusal surfaces as the launch's error
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    const dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (a.b.nx + XT_LX - 1) / XT_LX);
+    kern<<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[3]), a.U,
+                                          const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1],
+                                          (const double*)a.F[2], a.V, a.vs, a.b, a.fb[1], a.fb[2], a.c, a.flags,
+                                          a.slot, LAST ? a.slot_next : nullptr, a.m1, a.m2, a.mc, a.clock, err);
+}
+
+template <bool CHAR, bool BORGES, bool PHYS>
+static void xt_h(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s) {
+    const int h = a.viscous ? 1 : 0;  // the viscous terms arrive precomputed; H only sizes the operands
+    if (a.slot_next) {
+        if (h) xt_launch<CHAR, BORGES, PHYS, 1, true>(a, m, err, s);
+        else xt_launch<CHAR, BORGES, PHYS, 0, true>(a, m, err, s);
+    } else {
+        if (h) xt_launch<CHAR, BORGES, PHYS, 1, false>(a, m, err, s);
+        else xt_launch<CHAR, BORGES, PHYS, 0, false>(a, m, err, s);
+    }
+}
+
+void launch_xface_update_tma(bool chr, bool borges, const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err,
+                             cudaStream_t s) {
+    if (chr) {
+        if (borges) { if (a.phys) xt_h<true, true, true>(a, m, err, s); else xt_h<true, true, false>(a, m, err, s); }
+        else { if (a.phys) xt_h<true, false, true>(a, m, err, s); else xt_h<true, false, false>(a, m, err, s); }
+    } else {
+        if (borges) { if (a.phys) xt_h<false, true, true>(a, m, err, s); else xt_h<false, true, false>(a, m, err, s); }
+        else { if (a.phys) xt_h<false, false, true>(a, m, err, s); else xt_h<false, false, false>(a, m, err, s); }
     }
 }
 
