@@ -279,8 +279,8 @@ COMPUTE_PER_UNIT = {
     ("reference", "fp64_char", "face_z"): (1395, 1003, "fp64", "face"),
     ("reference", "fp64_comp", "face_y"): (1041, 789, "fp64", "face"),
     ("reference", "fp64_comp", "face_z"): (1041, 789, "fp64", "face"),
-    ("reference", "fp64_char", "xface_update"): (1527, 1097, "fp64", "cell"),
-    ("reference", "fp64_comp", "xface_update"): (1178, 872, "fp64", "cell"),
+    ("reference", "fp64_char", "xface_update"): (1550, 1108, "fp64", "cell"),
+    ("reference", "fp64_comp", "xface_update"): (1161, 859, "fp64", "cell"),
     ("reference", "fp64_char", "viscous"): (222, 136, "fp64", "cell"),
     ("reference", "fp64_comp", "viscous"): (222, 136, "fp64", "cell"),
     ("reference", "fp32_char", "stage_fused"): (4216, 2885, "fp32", "cell"),
@@ -289,8 +289,8 @@ COMPUTE_PER_UNIT = {
     ("physical", "fp64_char", "face_z"): (1441, 1032, "fp64", "face"),
     ("physical", "fp64_comp", "face_y"): (1078, 802, "fp64", "face"),
     ("physical", "fp64_comp", "face_z"): (1078, 802, "fp64", "face"),
-    ("physical", "fp64_char", "xface_update"): (1638, 1166, "fp64", "cell"),
-    ("physical", "fp64_comp", "xface_update"): (1255, 923, "fp64", "cell"),
+    ("physical", "fp64_char", "xface_update"): (1614, 1149, "fp64", "cell"),
+    ("physical", "fp64_comp", "xface_update"): (1237, 909, "fp64", "cell"),
     ("physical", "fp64_char", "viscous"): (369, 202, "fp64", "cell"),
     ("physical", "fp64_comp", "viscous"): (369, 202, "fp64", "cell"),
     ("physical", "fp32_char", "stage_fused"): (4486, 3070, "fp32", "cell"),
@@ -303,20 +303,20 @@ COMPUTE_PER_UNIT = {
 TRAFFIC_PER_UNIT = {
     ("reference", "fp64_char", "face_y"): 68.6, ("reference", "fp64_char", "face_z"): 65.7,
     ("reference", "fp64_comp", "face_y"): 66.0, ("reference", "fp64_comp", "face_z"): 63.2,
-    ("reference", "fp64_char", "xface_update"): 330.2, ("reference", "fp64_comp", "xface_update"): 327.8,
+    ("reference", "fp64_char", "xface_update"): 321.2, ("reference", "fp64_comp", "xface_update"): 320.7,
     ("reference", "fp64_char", "viscous"): 51.2, ("reference", "fp64_comp", "viscous"): 51.2,
     ("reference", "fp64_char", "fill_prim"): 21.8, ("reference", "fp64_comp", "fill_prim"): 21.7,
     ("reference", "fp32_char", "stage_fused"): 119.2, ("reference", "fp32_comp", "stage_fused"): 119.4,
     ("physical", "fp64_char", "face_y"): 67.3, ("physical", "fp64_char", "face_z"): 65.3,
     ("physical", "fp64_comp", "face_y"): 65.1, ("physical", "fp64_comp", "face_z"): 62.5,
-    ("physical", "fp64_char", "xface_update"): 329.5, ("physical", "fp64_comp", "xface_update"): 328.9,
+    ("physical", "fp64_char", "xface_update"): 320.9, ("physical", "fp64_comp", "xface_update"): 320.7,
     ("physical", "fp64_char", "viscous"): 61.6, ("physical", "fp64_comp", "viscous"): 61.7,
     ("physical", "fp64_char", "fill_prim"): 21.6, ("physical", "fp64_comp", "fill_prim"): 21.9,
     ("physical", "fp32_char", "stage_fused"): 118.9, ("physical", "fp32_comp", "stage_fused"): 119.0,
 }
 KERNEL_NAMES = {"stage_fused": "k_stage_march", "update": "k_update",
                 "sensor": "k_sensor_prims + k_sensor_mask_tc + k_gate_delta/k_gate_apply",
-                "xface_update": "k_xface_update", "viscous": "k_viscous", "fill_prim": "k_fill_prim/k_fill_halo",
+                "xface_update": "k_xface_update_tma", "viscous": "k_viscous", "fill_prim": "k_fill_prim/k_fill_halo",
                 "step_begin": "k_step_begin", "face_x": "k_face_flux<x>", "face_y": "k_face_flux<y>",
                 "face_z": "k_face_flux<z>"}
 
