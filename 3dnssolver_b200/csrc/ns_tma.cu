@@ -11,6 +11,10 @@
 // leave the warps' critical path (the per-thread kernel k_face_flux waits on
 // its 30 global loads per face).  The face arithmetic is the same code
 // (face_stencil_from + face_comp/face_char), so the fluxes are bit-identical.
+// (A pass that formed U, the half flux and the wave speed once per cell of the
+// tile in shared memory, instead of once per face through the cell, ran 2-6%
+// slower on B200 at 256^3: the extra barrier and shared-memory traffic cost
+// more than the 12-15% of FP64 operations it saved.)
 //
 // Tiles (halo'd coordinates; TMA wants the innermost start x 8 bytes and the
 // box's innermost extent x 8 bytes to be multiples of 16):
@@ -56,27 +60,12 @@ struct FaceTile<2> {
     static constexpr int SS = 1;
 };
 
-// Per-cell precompute (NS_FACE_PRE, on by default): after a tile lands, the
-// block forms once per cell the quantities every face through it needs -- U =
-// cons(W), half the Euler flux along DIR and the local wave speed |q_n| + c --
-// into shared memory, instead of each of the 6 faces through the cell forming
-// them again (the same expressions, so the fluxes keep their bits).
-#ifndef NS_FACE_PRE
-#define NS_FACE_PRE 1
-#endif
-
 template <int DIR>
 struct FaceTileDims {
     static constexpr int QS = FaceTile<DIR>::BY * FaceTile<DIR>::BZ;  // one field of the box
     static constexpr int ELEMS = 5 * QS;
     static constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // buffers 128-byte aligned
     static constexpr uint32_t BYTES = ELEMS * 8;
-    // the cells the faces read: y-faces all 9 rows x columns 1..32, z-faces the
-    // 4 rows x columns 0..36
-    static constexpr int PCOLS = DIR == 1 ? 32 : 37, PCOL0 = DIR == 1 ? 1 : 0;
-    static constexpr int NCELL = FaceTile<DIR>::BY * PCOLS;
-    static constexpr int NPRE = 11;  // U (5), half flux (5), |q_n| + c (1)
-    static constexpr size_t smem = (size_t)(2 * STRIDE + (NS_FACE_PRE ? NPRE * QS : 0)) * 8;
 };
 
 template <bool CHAR>
@@ -92,33 +81,19 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
                     unsigned long long* __restrict__ err) {
     using FT = FaceTile<DIR>;
     using TD = FaceTileDims<DIR>;
-    constexpr bool PRE = NS_FACE_PRE;
-    extern __shared__ __align__(128) double fsm[];
-    double* buf = fsm;                    // [2][5][BY][BZ] W tiles
-    double* pre = fsm + 2 * TD::STRIDE;   // [11][BY][BZ] per-cell U, half flux, wave speed
+    __shared__ __align__(128) double buf[2 * TD::STRIDE];
     __shared__ __align__(8) unsigned long long full[2];
     const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
     const int nzt = (b.nz + 31) / 32, nyt = (b.ny + 3) / 4;
     const int tiles = b.nx * nyt * nzt;  // the host keeps this below 2^31
     const int G = gridDim.x;
     const uint32_t bar[2] = {tc::smem_u32(&full[0]), tc::smem_u32(&full[1])};
-    const double gamma = c.gamma, half = 0.5;
-    const double hg = half * gamma * c.inv_gm1;
     auto issue = [&](int t, int s) {
         const int tz = t % nzt, r = t / nzt, tyi = r % nyt, aa = r / nyt;
         const int kk0 = tz * 32, bb0 = tyi * 4;
         mbar_expect_tx(bar[s], TD::BYTES);
         tma_load_4d(tc::smem_u32(buf + s * TD::STRIDE), &map, DIR == 1 ? kk0 + 2 : kk0, DIR == 1 ? bb0 : bb0 + 3,
                     aa + NG, 0, bar[s]);
-    };
-    auto fail = [&](int t, int it, int s, uint32_t par) {
-        if (tid == 0) {
-            atomicOr(err, 1ull);
-            // the copies in flight: this tile's (buffer s) and the next one's (buffer s ^ 1)
-            tc::mbar_wait(bar[s], par, kTilePolls);
-            if (t + G < tiles) tc::mbar_wait(bar[s ^ 1], ((it + 1) >> 1) & 1, kTilePolls);
-        }
-        __syncthreads();
     };
     if (tid == 0) {
         tc::mbar_init(bar[0], 1);
@@ -134,79 +109,18 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
         const int s = it & 1;
         const uint32_t par = (it >> 1) & 1;
         const bool ok = tc::mbar_wait(bar[s], par, kTilePolls);
-        const double* Wt = buf + s * TD::STRIDE;
-        if constexpr (PRE) {
-            if (ok) {
-                for (int e = tid; e < TD::NCELL; e += 128) {
-                    const int o = (e / TD::PCOLS) * FT::BZ + TD::PCOL0 + e % TD::PCOLS;
-                    double w[5], u[5], f[5];
-#pragma unroll
-                    for (int q = 0; q < 5; q++) w[q] = Wt[q * TD::QS + o];
-                    cons_from_prim(w, c.inv_gm1, u);
-                    half_flux<DIR, double>(w, hg, f);
-#pragma unroll
-                    for (int q = 0; q < 5; q++) {
-                        pre[q * TD::QS + o] = u[q];
-                        pre[(5 + q) * TD::QS + o] = f[q];
-                    }
-                    if constexpr (PHYS) {
-                        const double gp = gamma * w[1];
-                        pre[10 * TD::QS + o] = fabs(w[2 + DIR]) + gp * trsqrt(gp * w[0]);
-                    }
-                }
-            }
-            if (__syncthreads_or(!ok)) {
-                fail(t, it, s, par);
-                return;
-            }
-        }
         if (ok) {
             const int tz = t % nzt, r = t / nzt, tyi = r % nyt, aa = r / nyt;
             const int kk = tz * 32 + lane, bb = tyi * 4 + ty;
             if (kk < b.nz && bb < b.ny) {
-                const int c0 = ty * FT::BZ + FT::Z0 + lane;  // stencil cell 0
+                const double* sm = buf + s * TD::STRIDE + ty * FT::BZ + FT::Z0 + lane;
+                auto ld = [&](int st, double w[5], double u[5]) {
+#pragma unroll
+                    for (int q = 0; q < 5; q++) w[q] = sm[q * TD::QS + st * FT::SS];
+                    cons_from_prim(w, c.inv_gm1, u);
+                };
                 double fL[5][5], fR[5][5], wa[5], out[5];
-                if constexpr (PRE) {
-                    // face_stencil_from's split from the precomputed cells
-                    double halpha = 1.5;
-                    if constexpr (PHYS) {
-                        double amax = 0.0;
-#pragma unroll
-                        for (int st = 0; st < 6; st++) {
-                            const double a = pre[10 * TD::QS + c0 + st * FT::SS];
-                            amax = (st == 0) ? a : (a > amax ? a : amax);
-                        }
-                        halpha = half * amax;
-                    }
-#pragma unroll
-                    for (int st = 0; st < 6; st++) {
-                        const int o = c0 + st * FT::SS;
-                        if constexpr (CHAR) {
-                            if (st == 2) {
-#pragma unroll
-                                for (int q = 0; q < 5; q++) wa[q] = Wt[q * TD::QS + o];
-                            }
-                            if (st == 3) {
-#pragma unroll
-                                for (int q = 0; q < 5; q++) wa[q] = half * (wa[q] + Wt[q * TD::QS + o]);
-                            }
-                        }
-#pragma unroll
-                        for (int q = 0; q < 5; q++) {
-                            const double u = pre[q * TD::QS + o], f = pre[(5 + q) * TD::QS + o];
-                            if (st <= 4) fL[q][st] = halpha * u + f;
-                            if (st >= 1) fR[q][st - 1] = f - halpha * u;
-                        }
-                    }
-                } else {
-                    const double* sm = Wt + c0;
-                    auto ld = [&](int st, double w[5], double u[5]) {
-#pragma unroll
-                        for (int q = 0; q < 5; q++) w[q] = sm[q * TD::QS + st * FT::SS];
-                        cons_from_prim(w, c.inv_gm1, u);
-                    };
-                    face_stencil_from<DIR, CHAR, PHYS, double>(ld, c, fL, fR, wa);
-                }
+                face_stencil_from<DIR, CHAR, PHYS, double>(ld, c, fL, fR, wa);
                 if constexpr (!CHAR)
                     face_comp<double, BORGES>(fL, fR, out);
                 else
@@ -216,10 +130,15 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
                 for (int q = 0; q < 5; q++) F[q * fb.fstride + fo] = out[q];
             }
         }
-        // every thread is done with buffer s and the precomputed cells (and agrees on
-        // whether a wait ran out)
+        // every thread is done with buffer s (and agrees on whether a wait ran out)
         if (__syncthreads_or(!ok)) {
-            fail(t, it, s, par);
+            if (tid == 0) {
+                atomicOr(err, 1ull);
+                // the copies in flight: this tile's (buffer s) and the next one's (buffer s ^ 1)
+                tc::mbar_wait(bar[s], par, kTilePolls);
+                if (t + G < tiles) tc::mbar_wait(bar[s ^ 1], ((it + 1) >> 1) & 1, kTilePolls);
+            }
+            __syncthreads();
             return;
         }
         if (tid == 0 && t + 2 * G < tiles) issue(t + 2 * G, s);
@@ -439,11 +358,7 @@ static void tma_one(const WTmaMaps& m, const Box& b, const Consts& c, double* F,
     const int tiles = b.nx * ((b.ny + 3) / 4) * ((b.nz + 31) / 32);
     const int grid = std::min(tiles, sms * TmaFaceMinBlocks<CHAR>::value);
     const CUtensorMap& map = *reinterpret_cast<const CUtensorMap*>(m.map[DIR - 1]);
-    constexpr size_t bytes = FaceTileDims<DIR>::smem;
-    auto kern = k_face_flux_tma<DIR, CHAR, BORGES, PHYS>;
-    // the attribute is per device; a refusal surfaces as the launch's error
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    kern<<<grid, dim3(32, 4), bytes, s>>>(map, b, c, F, fb, err);
+    k_face_flux_tma<DIR, CHAR, BORGES, PHYS><<<grid, dim3(32, 4), 0, s>>>(map, b, c, F, fb, err);
 }
 
 template <int DIR>
