@@ -264,13 +264,13 @@ static void prof_mark(ns_ctx* ctx, int cls) {
     g_prof->cls[g_prof->n++] = cls;
 }
 
-// TMA-staged FP64 kernels: the y/z faces and the CD-2 viscous terms of the
-// physical semantics (build switches, on by default)
+// TMA-staged FP64 kernels: the y/z faces and the viscous terms of the physical
+// semantics, the x-march of both (build switches, on by default)
 #ifndef NS_FACE_TMA
 #define NS_FACE_TMA 1
 #endif
-#ifndef NS_VISC_TMA
-#define NS_VISC_TMA 1
+#ifndef NS_VISC_TMA_MAX_ORDER
+#define NS_VISC_TMA_MAX_ORDER 6  // CD orders whose physical viscous terms march over TMA planes
 #endif
 #ifndef NS_XUPD_TMA
 #define NS_XUPD_TMA 1
@@ -495,9 +495,9 @@ static ns_status do_step(ns_ctx* ctx) {
             a.V = (const double*)ctx->F[0];
             a.vs = ctx->fb[0].fstride;
             const nsb::WTmaMaps* m = tma_maps(ctx);
-            if (NS_VISC_TMA && m && phys(ctx) && ctx->c.order == 2)
-                launch_viscous_tma(*m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0], ctx->fb[0].fstride,
-                                   ctx->slot + 4, s);
+            if (m && phys(ctx) && ctx->c.order <= NS_VISC_TMA_MAX_ORDER)
+                launch_viscous_tma(ctx->c.order / 2, *m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
+                                   ctx->fb[0].fstride, ctx->slot + 4, s);
             else
                 launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
                                ctx->fb[0].fstride, s);
@@ -829,6 +829,8 @@ ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out) {
     return NS_OK;
 }
 
+static ns_status device_status(ns_ctx* ctx);
+
 ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
     if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
     if (!W) return fail(NS_ERR_INVALID_ARG, "W is NULL");
@@ -844,6 +846,7 @@ ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
     NS_TRY(download(ctx, ctx->W, W));
     if (U) NS_TRY(download(ctx, ctx->U, U));
     if (dt_out) *dt_out = clk[0];
+    NS_TRY(device_status(ctx));
     return check_state(ctx);
 }
 
@@ -865,14 +868,22 @@ ns_status ns_get_dt(ns_ctx* ctx, double* dt, double* time) {
     return NS_OK;
 }
 
-ns_status ns_synchronize(ns_ctx* ctx) {
-    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
-    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+// the status words of the device's bounded waits and self-checks (after the
+// stream is idle)
+static ns_status device_status(ns_ctx* ctx) {
     if (ctx->sensor && sensor_status(ctx->sensor) != NS_OK)
         return fail(NS_ERR_TIMEOUT, "a tensor-core wait of the sensor's flag kernel ran out of polls");
     unsigned long long werr = 0;
     NS_CUDA(cudaMemcpy(&werr, ctx->slot + 4, sizeof werr, cudaMemcpyDeviceToHost));
-    if (werr) return fail(NS_ERR_TIMEOUT, "a TMA tile wait of a face or viscous kernel ran out of polls");
+    if (werr & 2) return fail(NS_ERR_CUDA, "a TMA kernel found its shared-memory ring misaligned and did nothing");
+    if (werr) return fail(NS_ERR_TIMEOUT, "a TMA tile wait of a face, x-march or viscous kernel ran out of polls");
+    return NS_OK;
+}
+
+ns_status ns_synchronize(ns_ctx* ctx) {
+    if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
+    NS_CUDA(cudaStreamSynchronize(ctx->stream));
+    NS_TRY(device_status(ctx));
     return check_state(ctx);
 }
 

@@ -658,88 +658,115 @@ __global__ void __launch_bounds__(128) k_viscous(const double* __restrict__ W, B
     for (int q = 1; q < 5; q++) V[(q - 1) * vs + e] = rv[q];
 }
 
-// Physical semantics, CD-2: the same terms from planes of W that the TMA unit
-// loads into a 4-slot ring while the block marches VISC_LX cells along x.  A
-// block owns 4 rows x 32 columns; one plane is the box z = k0-1 .. k0+32,
-// rows j0-1 .. j0+4 (34 x 6 x 5 fields, halo'd coordinates from k0+2, an even
-// start as TMA requires), so each cell of W crosses L2 once per block instead
-// of once per stencil.  A cell on a domain edge line (at the boundary along
-// two axes or more) needs folded corner cells for its mixed derivatives, which
-// no fill writes and so the box does not hold: it reads the device state like
-// k_viscous.  Waits are bounded (the error word receives 1 and the block ends).
+// Physical semantics: the same terms from planes of W that the TMA unit loads
+// into a ring while the block marches VISC_LX cells along x.  A block owns 4
+// rows x 32 columns; one plane is the box of ViscTile<H> (5 fields; 8.2, 12.2
+// and 15.2 KB for CD-2, 4, 6), so each cell of W crosses L2 once per block
+// instead of once per stencil.  The ring holds the 2H+1 planes of the current
+// cell and, for CD-2 and CD-4, the next plane in flight; CD-6 keeps 7 slots
+// (two blocks per SM) and loads the next plane as the last one is released.
+// A cell within H cells of the boundary along two axes or more needs folded
+// edge or corner ghost cells for its mixed derivatives, which no fill writes
+// and so the box does not hold: it reads the device state like k_viscous.  Waits are
+// bounded (the error word receives 1 and the block ends).
 constexpr int VISC_LX = 32;
 
-__global__ void __launch_bounds__(128, 4)
+template <int H>
+struct ViscRing {
+    using VT = ViscTile<H>;
+    static constexpr int QS = VT::BZ * VT::BY, ELEMS = 5 * QS;
+    static constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // 128-byte aligned slots
+    static constexpr uint32_t BYTES = ELEMS * 8;
+    static constexpr int LEAD = H < 3 ? 1 : 0;             // planes in flight beyond the stencil
+    static constexpr int NSLOT = 2 * H + 1 + LEAD;
+    // the ring, then its mbarriers: no static shared memory, so the dynamic ring
+    // starts at the window's base (TMA writes want 128-byte aligned destinations)
+    static constexpr size_t smem = (size_t)NSLOT * STRIDE * 8 + NSLOT * 8;
+    static constexpr int MINB = H == 1 ? 4 : (H == 2 ? 3 : 2);
+};
+
+template <int H>
+__global__ void __launch_bounds__(128, ViscRing<H>::MINB)
     k_viscous_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ W, Box b, Consts c,
                   double* __restrict__ V, long long vs, unsigned long long* __restrict__ err) {
-    constexpr int BZ = VISC_TMA_BZ, BY = VISC_TMA_BY, QS = BZ * BY, ELEMS = 5 * QS;
-    constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // 128-byte aligned slots
-    constexpr uint32_t BYTES = ELEMS * 8;
-    constexpr int NSLOT = 4;
-    __shared__ __align__(128) double ring[NSLOT * STRIDE];
-    __shared__ __align__(8) unsigned long long full[NSLOT];
+    using VT = ViscTile<H>;
+    using VR = ViscRing<H>;
+    constexpr int NSLOT = VR::NSLOT, STRIDE = VR::STRIDE, QS = VR::QS, BZ = VT::BZ;
+    extern __shared__ __align__(128) double vring[];  // [NSLOT][5][BY][BZ], then NSLOT mbarriers
+    unsigned long long* full = reinterpret_cast<unsigned long long*>(vring + NSLOT * STRIDE);
     const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
+    if (tc::smem_u32(vring) & 127u) {  // a TMA destination must be 128-byte aligned: report, touch nothing
+        if (tid == 0) atomicOr(err, 2ull);
+        return;
+    }
     const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = blockIdx.z * VISC_LX;
     const int x1 = min(x0 + VISC_LX, b.nx);
     const int k = k0 + lane, j = j0 + ty;
     const bool live = k < b.nz && j < b.ny;
-    // plane p (x0 - 1 <= p <= x1) is the (p - x0 + 1)-th load of the block
-    auto slot = [&](int p) { return (p - x0 + 1) % NSLOT; };
+    // plane p (x0 - H <= p <= x1 - 1 + H) is the (p - x0 + H)-th load of the block
+    auto slot = [&](int p) { return (p - x0 + H) % NSLOT; };
     auto bar = [&](int p) { return tc::smem_u32(&full[slot(p)]); };
-    auto par = [&](int p) { return (uint32_t)(((p - x0 + 1) / NSLOT) & 1); };
+    auto par = [&](int p) { return (uint32_t)(((p - x0 + H) / NSLOT) & 1); };
     auto issue = [&](int p) {
-        mbar_expect_tx(bar(p), BYTES);
-        tma_load_4d(tc::smem_u32(ring + slot(p) * STRIDE), &map, k0 + 2, j0 + 2, p + NG, 0, bar(p));
+        mbar_expect_tx(bar(p), VR::BYTES);
+        tma_load_4d(tc::smem_u32(vring + slot(p) * STRIDE), &map, k0 + VT::Z0, j0 + NG - H, p + NG, 0, bar(p));
     };
     if (tid == 0)
         for (int q = 0; q < NSLOT; q++) tc::mbar_init(tc::smem_u32(&full[q]), 1);
     __syncthreads();
-    const int pre = min(x0 + 2, x1);  // planes in flight before the march
+    const int last = x1 - 1 + H;  // the last plane the block reads
     if (tid == 0)
-        for (int p = x0 - 1; p <= pre; p++) issue(p);
-    bool ok = tc::mbar_wait(bar(x0 - 1), par(x0 - 1), kTilePolls);
-    ok = ok && tc::mbar_wait(bar(x0), par(x0), kTilePolls);
-    const int nbjk = (j == 0 || j == b.ny - 1) + (k == 0 || k == b.nz - 1);
-    const int cc = (ty + 1) * BZ + lane + 1;
-    int waited = x0;  // planes up to this one have landed
+        for (int p = x0 - H; p <= min(x0 + H + VR::LEAD, last); p++) issue(p);
+    bool ok = true;
+    for (int p = x0 - H; p < x0 + H; p++) ok = ok && tc::mbar_wait(bar(p), par(p), kTilePolls);
+    int waited = ok ? x0 + H - 1 : x0 - H - 1;  // planes up to this one have landed
+    // within H cells of the boundary along two axes or more, a mixed derivative
+    // reaches an edge or corner ghost cell
+    const int nbjk = (j < H || j >= b.ny - H) + (k < H || k >= b.nz - H);
+    const int cc = (ty + H) * BZ + lane + VT::C0;
     for (int i = x0; i < x1; i++) {
-        ok = ok && tc::mbar_wait(bar(i + 1), par(i + 1), kTilePolls);
-        if (ok) waited = i + 1;
+        if (ok && i + H > waited) {
+            ok = tc::mbar_wait(bar(i + H), par(i + H), kTilePolls);
+            if (ok) waited = i + H;
+        }
         if (ok && live) {
             double rv[5] = {0, 0, 0, 0, 0};
-            if (nbjk + (i == 0 || i == b.nx - 1) >= 2) {
-                viscous_physical<1, double>(W, b, c, i, j, k, rv);
+            if (nbjk + (i < H || i >= b.nx - H) >= 2) {
+                viscous_physical<H, double>(W, b, c, i, j, k, rv);
             } else {
-                const double* P[3] = {ring + slot(i - 1) * STRIDE, ring + slot(i) * STRIDE,
-                                      ring + slot(i + 1) * STRIDE};
-                auto at = [&](int q, int ox, int oy, int oz) { return P[1 + ox][q * QS + cc + oy * BZ + oz]; };
+                const double* P[2 * H + 1];
+#pragma unroll
+                for (int s = 0; s <= 2 * H; s++) P[s] = vring + slot(i - H + s) * STRIDE;
+                auto at = [&](int q, int ox, int oy, int oz) { return P[H + ox][q * QS + cc + oy * BZ + oz]; };
                 auto ld1 = [&](int q, int ax, int t) {
-                    const int d = t - 1;
+                    const int d = t - H;
                     return at(q, ax == 0 ? d : 0, ax == 1 ? d : 0, ax == 2 ? d : 0);
                 };
                 auto ld2 = [&](int q, int a, int s, int bx, int t) {
                     int o[3] = {0, 0, 0};
-                    o[a] += s - 1;
-                    o[bx] += t - 1;
+                    o[a] += s - H;
+                    o[bx] += t - H;
                     return at(q, o[0], o[1], o[2]);
                 };
-                viscous_physical_core<1, double>(ld1, ld2, c, rv);
+                viscous_physical_core<H, double>(ld1, ld2, c, rv);
             }
             const long long e = ((long long)i * b.ny + j) * b.nz + k;
 #pragma unroll
             for (int q = 1; q < 5; q++) V[(q - 1) * vs + e] = rv[q];
         }
-        // every thread is done with plane i - 1 (and agrees on whether a wait ran out)
+        // every thread is done with plane i - H (and agrees on whether a wait ran out)
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 atomicOr(err, 1ull);
-                // the loads still in flight: planes waited + 1 .. min(i + 2, x1)
-                for (int p = waited + 1; p <= min(i + 2, x1); p++) tc::mbar_wait(bar(p), par(p), kTilePolls);
+                // the loads still in flight: planes waited + 1 .. the last one issued
+                const int issued = min(i + H + VR::LEAD, last);
+                for (int p = waited + 1; p <= issued; p++) tc::mbar_wait(bar(p), par(p), kTilePolls);
             }
             __syncthreads();
             return;
         }
-        if (tid == 0 && i + 3 <= x1) issue(i + 3);  // into the slot of plane i - 1
+        const int next = i + H + 1 + VR::LEAD;  // into the slot of plane i - H
+        if (tid == 0 && next <= last) issue(next);
     }
 }
 
@@ -1218,11 +1245,22 @@ static void visc_one(const double* W, const Box& b, const Consts& c, double* V, 
     k_viscous<H, PHYS><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, V, vs);
 }
 
-void launch_viscous_tma(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
-                        long long vs, unsigned long long* err, cudaStream_t s) {
+template <int H>
+static void visc_tma_one(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V, long long vs,
+                         unsigned long long* err, cudaStream_t s) {
+    constexpr size_t bytes = ViscRing<H>::smem;
+    // the attribute is per device; a refusal surfaces as the launch's error
+    cudaFuncSetAttribute(k_viscous_tma<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     const dim3 grid((b.nz + 31) / 32, (b.ny + 3) / 4, (b.nx + VISC_LX - 1) / VISC_LX);
-    k_viscous_tma<<<grid, dim3(32, 4), 0, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[2]), W, b, c, V, vs,
-                                               err);
+    k_viscous_tma<H><<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[3 + H - 1]), W, b,
+                                                       c, V, vs, err);
+}
+
+void launch_viscous_tma(int h, const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
+                        long long vs, unsigned long long* err, cudaStream_t s) {
+    if (h == 1) visc_tma_one<1>(m, W, b, c, V, vs, err, s);
+    else if (h == 2) visc_tma_one<2>(m, W, b, c, V, vs, err, s);
+    else visc_tma_one<3>(m, W, b, c, V, vs, err, s);
 }
 
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,

@@ -101,16 +101,25 @@ void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, cons
 void launch_face_tail_w(int dir, bool chr, bool borges, bool phys, const double* W, const Box& b,
                         const Consts& c, void* F, const FaceBox& fb, cudaStream_t s);
 // TMA tensor maps of one W buffer (ns_tma.cu): map[0] the y-face tiles, map[1]
-// the z-face tiles, map[2] the planes of the marched viscous kernel, map[3] the
-// x-march's planes; each holds a CUtensorMap (128 bytes, 64-byte aligned)
+// the z-face tiles, map[2] the x-march's planes, map[3 + h - 1] the planes of the
+// marched viscous kernel of half-width h (CD-2h); each holds a CUtensorMap
+// (128 bytes, 64-byte aligned)
 struct WTmaMaps {
-    alignas(64) unsigned char map[4][128];
+    alignas(64) unsigned char map[6][128];
     const double* W = nullptr;
     bool ok = false;
 };
-// box of one plane of the TMA-marched viscous kernel (CD-2): z from kk0 + 2
-// (halo'd, even) 34 wide, rows j0 + 2 .. j0 + 7
-constexpr int VISC_TMA_BZ = 34, VISC_TMA_BY = 6;
+// one plane of the TMA-marched viscous kernel of half-width H for a block of
+// 4 rows x 32 columns (halo'd coordinates): rows j0+3-H .. j0+6+H, columns from
+// k0+3-H rounded down to even (TMA's innermost start rule), 32 + 2H (+1) wide
+// rounded up to even; lane 0's cell sits in column C0
+template <int H>
+struct ViscTile {
+    static constexpr int Z0 = (3 - H) & ~1;          // box start minus k0
+    static constexpr int C0 = 3 - Z0;                // lane 0's cell column in the box
+    static constexpr int BZ = (C0 + 32 + H + 1) & ~1;  // columns
+    static constexpr int BY = 4 + 2 * H;             // rows
+};
 // false (and m->ok false) where TMA cannot serve the buffer: no driver entry
 // point, an unaligned base or too many tiles; the per-thread kernels then run
 bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b);
@@ -130,9 +139,9 @@ void launch_xface_update_tma(bool chr, bool borges, const UpdateArgs& a, const W
 // vs >= nx ny nz), half-width h = order/2 of the centered scheme
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
                     long long vs, cudaStream_t s);
-// the same for physical semantics and CD-2 from TMA-loaded planes of the W that
-// m maps, marched along x; *err receives 1 if a wait ran out
-void launch_viscous_tma(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
+// the same for physical semantics from TMA-loaded planes of the W that m maps,
+// marched along x (half-width h = 1, 2, 3); *err receives 1 if a wait ran out
+void launch_viscous_tma(int h, const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
                         long long vs, unsigned long long* err, cudaStream_t s);
 // slab halo exchange: pack the outer interior planes of a side / unpack into its ghost planes
 void launch_slab_pack(const double* U, const Box& b, int side, double* buf, cudaStream_t s);

@@ -183,6 +183,10 @@ __global__ void __launch_bounds__(128, 2)
     double* opnd = fprev + 5 * 128;                  // [NOP][128]
     unsigned long long* full = reinterpret_cast<unsigned long long*>(opnd + XL::NOP * 128);
     const int lane = threadIdx.x, ty = threadIdx.y, t = ty * 32 + lane;
+    if (tc::smem_u32(ring) & 127u) {  // a TMA destination must be 128-byte aligned: report, touch nothing
+        if (t == 0) atomicOr(err, 2ull);
+        return;
+    }
     const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = blockIdx.z * XT_LX;
     const int k = k0 + lane, j = j0 + ty;
     const int x1 = min(x0 + XT_LX, b.nx);
@@ -337,10 +341,12 @@ bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b) {
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const cuuint32_t box1[4] = {FaceTile<1>::BZ, FaceTile<1>::BY, 1, 5};
     const cuuint32_t box2[4] = {FaceTile<2>::BZ, FaceTile<2>::BY, 1, 5};
-    const cuuint32_t boxv[4] = {VISC_TMA_BZ, VISC_TMA_BY, 1, 5};
     const cuuint32_t boxx[4] = {XTmaLayout<0>::BZ, XTmaLayout<0>::BY, 1, 5};
-    const cuuint32_t* boxes[4] = {box1, box2, boxv, boxx};
-    for (int d = 0; d < 4; d++) {
+    const cuuint32_t boxv1[4] = {ViscTile<1>::BZ, ViscTile<1>::BY, 1, 5};
+    const cuuint32_t boxv2[4] = {ViscTile<2>::BZ, ViscTile<2>::BY, 1, 5};
+    const cuuint32_t boxv3[4] = {ViscTile<3>::BZ, ViscTile<3>::BY, 1, 5};
+    const cuuint32_t* boxes[6] = {box1, box2, boxx, boxv1, boxv2, boxv3};
+    for (int d = 0; d < 6; d++) {
         CUresult r = enc(reinterpret_cast<CUtensorMap*>(m->map[d]), CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4,
                          const_cast<double*>(W), dims, strides, boxes[d], estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -390,7 +396,7 @@ static void xt_launch(const UpdateArgs& a, const WTmaMaps& m, unsigned long long
     // the attribute is per device; a refusal surfaces as the launch's error
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     const dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (a.b.nx + XT_LX - 1) / XT_LX);
-    kern<<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[3]), a.U,
+    kern<<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[2]), a.U,
                                           const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1],
                                           (const double*)a.F[2], a.V, a.vs, a.b, a.fb[1], a.fb[2], a.c, a.flags,
                                           a.slot, LAST ? a.slot_next : nullptr, a.m1, a.m2, a.mc, a.clock, err);

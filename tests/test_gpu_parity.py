@@ -224,11 +224,13 @@ def test_physical_semantics_rhs_matches_oracle(oracle, shape, conv, order, bc, d
     assert ok.all(), f"rel L2 per field {err}"
 
 
-# the FP64 physical steps run the TMA-staged y/z face kernels and, with CD-2, the
-# TMA-marched viscous kernel: odd and partial tiles, domain edge lines (Neumann
-# and periodic), several x-blocks of the viscous march, 2D
+# the FP64 physical steps run the TMA-staged y/z face kernels, the TMA x-march
+# and the TMA-marched viscous kernel (CD-2/4/6): odd and partial tiles, domain
+# edge lines (Neumann and periodic), several x-blocks of the marches, 2D
 PHYS_STEP_CASES = [
     ((14, 12, 10), 3, 2, 4, (N, P, P)),
+    ((40, 10, 34), 3, 2, 4, (P, N, N)),
+    ((33, 11, 37), 3, 2, 6, (N, P, N)),
     ((19, 13, 35), 3, 2, 2, (N, N, N)),
     ((70, 6, 33), 3, 1, 2, (P, N, P)),
     ((21, 9, 1), 2, 2, 2, (N, P, P)),
