@@ -79,6 +79,7 @@ def load_library():
         "ns_sensor_predict": ([C, ctypes.c_longlong, fp, C, C], st),
         "ns_set_sensor_weights": ([C, fp], st),
         "ns_fma_peak": ([ctypes.c_int, dp], st),
+        "ns_wait_selftest": ([ctypes.c_uint, ctypes.POINTER(ctypes.c_int), dp], st),
         "ns_get_dt": ([C, dp, dp], st),
     }
     for name, (args, res) in protos.items():
@@ -129,6 +130,14 @@ def fma_peak(fp64=True):
     t = ctypes.c_double()
     _check(load_library().ns_fma_peak(1 if fp64 else 0, ctypes.byref(t)), "ns_fma_peak")
     return t.value
+
+
+def wait_selftest(polls=4096):
+    """Runs one bounded device wait on an mbarrier phase nothing completes;
+    returns (ran_out, ms): ran_out is True when the wait gave up as it must."""
+    r, t = ctypes.c_int(), ctypes.c_double()
+    _check(load_library().ns_wait_selftest(int(polls), ctypes.byref(r), ctypes.byref(t)), "ns_wait_selftest")
+    return bool(r.value), t.value
 
 
 def sensor_init(seed):

@@ -954,6 +954,34 @@ ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
 
 long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+ns_status ns_wait_selftest(unsigned polls, int* ran_out, double* ms) {
+    if (!ran_out || !ms) return fail(NS_ERR_INVALID_ARG, "ran_out and ms must be non-NULL");
+    if (polls == 0 || polls > (1u << 24)) return fail(NS_ERR_INVALID_ARG, "polls must lie in 1 .. 2^24");
+    unsigned long long* out = nullptr;
+    NS_CUDA(cudaMalloc(&out, sizeof *out));
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ns_status st = NS_OK;
+    unsigned long long h = 2;
+    float t = 0.f;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess || cudaMemsetAsync(out, 0xFF, sizeof *out, s) != cudaSuccess ||
+        cudaEventRecord(e0, s) != cudaSuccess || launch_wait_probe(polls, out, s) != cudaSuccess ||
+        cudaEventRecord(e1, s) != cudaSuccess ||
+        cudaMemcpyAsync(&h, out, sizeof h, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+        st = fail(NS_ERR_CUDA, "wait self-test failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+    cudaFree(out);
+    if (st != NS_OK) return st;
+    if (h > 1) return fail(NS_ERR_CUDA, "wait self-test wrote no result");
+    *ran_out = (int)h;
+    *ms = t;
+    return NS_OK;
+}
+
 ns_status ns_fma_peak(int fp64, double* tflops) {
     if (!tflops) return fail(NS_ERR_INVALID_ARG, "tflops is NULL");
     int dev = 0, sms = 0;

@@ -128,6 +128,9 @@ bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b);
 void launch_face_flux_tma(int dir, bool chr, bool borges, bool phys, const WTmaMaps& m, const double* W,
                           const Box& b, const Consts& c, void* F, const FaceBox& fb, int sms,
                           unsigned long long* err, cudaStream_t s);
+// one block waits (bounded) on an mbarrier phase nothing completes; out[0] = 1
+// if the wait gave up, 0 if it claimed completion
+cudaError_t launch_wait_probe(unsigned polls, unsigned long long* out, cudaStream_t s);
 void launch_update(const UpdateArgs& a, cudaStream_t s);
 // FP64 MODE_STAGE: x-faces + update in one march, U_out = a.Unext (a.F[0] unused)
 void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_t s);

@@ -313,6 +313,25 @@ __global__ void __launch_bounds__(128, 2)
     if constexpr (LAST) block_min_to(best, slot_next);
 }
 
+// The bounded wait of every TMA and tensor-core kernel, on a phase that no
+// arrival or transaction completes: it must give up after `polls` polls.
+__global__ void k_wait_probe(unsigned polls, unsigned long long* __restrict__ out) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) tc::mbar_init(tc::smem_u32(&bar), 1);
+    __syncthreads();
+    const bool done = tc::mbar_wait(tc::smem_u32(&bar), 0, polls);
+    if (__syncthreads_or(done)) {
+        if (threadIdx.x == 0) out[0] = 0;
+    } else if (threadIdx.x == 0) {
+        out[0] = 1;
+    }
+}
+
+cudaError_t launch_wait_probe(unsigned polls, unsigned long long* out, cudaStream_t s) {
+    k_wait_probe<<<1, 32, 0, s>>>(polls, out);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // host side
 

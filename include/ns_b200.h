@@ -303,6 +303,13 @@ NS_API ns_status ns_convection_solve_noalloc(const ns_params* p, const double* W
  * fp64 = 1 for double, 0 for float.  The denominator of the compute roofline
  * of the FMA-bound WENO kernels (no counterpart in the reference). */
 NS_API ns_status ns_fma_peak(int fp64, double* tflops);
+/* Self-test of the bounded device waits every TMA and tensor-core kernel uses:
+ * one block waits, at most `polls` polls, on an mbarrier phase that nothing
+ * completes.  *ran_out = 1 when the wait gave up and reported (the correct
+ * outcome), 0 if it claimed completion; *ms = the wait's device time.  The
+ * device stays usable afterwards (no fault, no trap).  No reference
+ * counterpart. */
+NS_API ns_status ns_wait_selftest(unsigned polls, int* ran_out, double* ms);
 /* Device kernels launched by this context since creation (for launch accounting). */
 NS_API long long ns_kernel_launches(ns_ctx* ctx);
 

@@ -85,3 +85,18 @@ def test_without_the_check_nan_propagates_silently_as_in_the_reference():
         d = s.diagnostics()
     assert d["nonfinite"]
     assert math.isfinite(d["dt"]) and d["dt"] > 0  # NaN never lowers the CFL minimum
+
+
+@pytest.mark.gpu
+def test_bounded_device_wait_gives_up_and_the_device_stays_usable():
+    """Every TMA and tensor-core kernel waits on mbarriers with a poll limit; a wait
+    on a phase that nothing completes must give up, report, and leave the context
+    usable (no fault, no trap)."""
+    ran_out, ms = pkg.wait_selftest(4096)
+    assert ran_out
+    assert ms < 1000.0
+    p = pkg.make_params(12, 10, 9, convection=pkg.CONV_WENO5_CHAR, mu=0.01)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(wl.random_field(p, seed=2))
+        s.advance(1)
+        s.synchronize()
