@@ -341,7 +341,8 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma, semantics):
     alg = BYTES_PER_CELL_STAGE * cells  # one stage of every cell per launch
     achieved = alg / (per_launch_ms / 1e3) / 1e9
     units = faces if dom.startswith("face") else cells
-    fkey = "fp64_char" if form.startswith("fp64_char") else form.split("_cd6")[0]
+    # CD-6/Borges forms have no counts of their own in the tables: no rows, not the CD-2 ones
+    fkey = form if "_cd6" in form else ("fp64_char" if form.startswith("fp64_char") else form)
     key = (sem, fkey, dom)
     tpu = TRAFFIC_PER_UNIT.get(key)
     traffic = round(tpu * units) if tpu else None
@@ -361,8 +362,8 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma, semantics):
     kname = KERNEL_NAMES.get(dom, dom)
     if sem == "physical" and dom in ("face_y", "face_z"):
         kname = kname.replace("k_face_flux", "k_face_flux_tma")
-    if sem == "physical" and dom == "viscous" and FORMS[form].get("order", 2) == 2:
-        kname = "k_viscous_tma"
+    if sem == "physical" and dom == "viscous":
+        kname = "k_viscous_tma<%d>" % (FORMS[form].get("order", 2) // 2)
     kname += f" ({form})"
     hbm = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
            "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
