@@ -52,6 +52,10 @@ namespace nsb {
 #ifndef NS_MARCH_TY
 #define NS_MARCH_TY 8
 #endif
+// cells a block marches along x
+#ifndef NS_MARCH_LX
+#define NS_MARCH_LX 32
+#endif
 //
 // Plane i reads planes i-2..i+3 (x-faces) and i-H..i+H (viscous terms).  With
 // H <= 1 ("lean") the ring holds 6 planes and the y/z face buffers alternate
@@ -68,7 +72,7 @@ namespace nsb {
 template <typename T, int H = 1>
 struct MarchTile {
     static_assert(sizeof(T) == 4, "the fused stage serves the FP32 form");
-    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = 32;
+    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = NS_MARCH_LX;
     static constexpr int FT = TY * TZ;  // threads per block, one per cell of the column
     static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
     static constexpr bool LEAN = H <= 1;

@@ -669,7 +669,10 @@ __global__ void __launch_bounds__(128) k_viscous(const double* __restrict__ W, B
 // edge or corner ghost cells for its mixed derivatives, which no fill writes
 // and so the box does not hold: it reads the device state like k_viscous.  Waits are
 // bounded (the error word receives 1 and the block ends).
-constexpr int VISC_LX = 32;
+#ifndef NS_VISC_LX
+#define NS_VISC_LX 32
+#endif
+constexpr int VISC_LX = NS_VISC_LX;
 
 template <int H>
 struct ViscRing {

@@ -156,7 +156,10 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
 // z-face fluxes, the viscous terms) still come per thread with cp.async, and
 // the update itself is k_xface_update's.  Two blocks per SM, so the
 // characteristic-wise face keeps its registers without spilling.
-constexpr int XT_LX = 32;
+#ifndef NS_XT_LX
+#define NS_XT_LX 32
+#endif
+constexpr int XT_LX = NS_XT_LX;
 
 template <int H>
 struct XTmaLayout {
