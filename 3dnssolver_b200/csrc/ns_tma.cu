@@ -68,11 +68,14 @@ struct FaceTileDims {
     static constexpr uint32_t BYTES = ELEMS * 8;
 };
 
+#ifndef NS_FACE_TMA_MINB_CHAR
+#define NS_FACE_TMA_MINB_CHAR 3
+#endif
 template <bool CHAR>
 struct TmaFaceMinBlocks {
     // as the per-thread kernels: 168 / 128 registers (2 blocks of 255-register
     // characteristic-wise threads ran 5% slower on B200)
-    static constexpr int value = CHAR ? 3 : 4;
+    static constexpr int value = CHAR ? NS_FACE_TMA_MINB_CHAR : 4;
 };
 
 template <int DIR, bool CHAR, bool BORGES, bool PHYS>
@@ -157,16 +160,20 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
 // the update itself is k_xface_update's.  Two blocks per SM, so the
 // characteristic-wise face keeps its registers without spilling.
 #ifndef NS_XT_LX
-#define NS_XT_LX 32
+#define NS_XT_LX 64
 #endif
+// Update operands: the characteristic-wise march stages all of them with
+// cp.async while its x-face is formed; the component-wise march stages U0 and U
+// only and reads the face fluxes and viscous terms at the update (8% faster
+// for it, 8% slower for the characteristic-wise march, B200 at 256^3).
 constexpr int XT_LX = NS_XT_LX;
 
-template <int H>
+template <int H, bool OPS = true>
 struct XTmaLayout {
     static constexpr int BZ = 34, BY = 4, QS = BZ * BY, ELEMS = 5 * QS;
     static constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // doubles per slot, 128-byte aligned
     static constexpr int NSLOT = 7;
-    static constexpr int NOP = H > 0 ? 34 : 30;
+    static constexpr int NOP = OPS ? (H > 0 ? 34 : 30) : 10;
     static constexpr uint32_t TX = ELEMS * 8;
     static constexpr size_t bytes = (size_t)(NSLOT * STRIDE + (5 + NOP) * 128) * 8 + NSLOT * 8;
 };
@@ -179,7 +186,8 @@ __global__ void __launch_bounds__(128, 2)
                        FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
                        unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
                        double* __restrict__ clock, unsigned long long* __restrict__ err) {
-    using XL = XTmaLayout<H>;
+    constexpr bool OPS = CHAR;  // every operand staged
+    using XL = XTmaLayout<H, OPS>;
     extern __shared__ __align__(128) unsigned char xsm[];
     double* ring = reinterpret_cast<double*>(xsm);  // [NSLOT][5][BY][BZ]
     double* fprev = ring + XL::NSLOT * XL::STRIDE;   // [5][128]
@@ -242,14 +250,16 @@ __global__ void __launch_bounds__(128, 2)
             for (int q = 0; q < 5; q++) {
                 cp_async8(&opnd[q * 128 + t], U0 + q * b.fstride + o);
                 cp_async8(&opnd[(5 + q) * 128 + t], U + q * b.fstride + o);
-                cp_async8(&opnd[(10 + q) * 128 + t], Fy + q * fy.fstride + fy.at(i, j, k));
-                cp_async8(&opnd[(15 + q) * 128 + t], Fy + q * fy.fstride + fy.at(i, j + 1, k));
-                if (convz) {
-                    cp_async8(&opnd[(20 + q) * 128 + t], Fz + q * fz.fstride + fz.at(i, j, k));
-                    cp_async8(&opnd[(25 + q) * 128 + t], Fz + q * fz.fstride + fz.at(i, j, k + 1));
+                if constexpr (OPS) {
+                    cp_async8(&opnd[(10 + q) * 128 + t], Fy + q * fy.fstride + fy.at(i, j, k));
+                    cp_async8(&opnd[(15 + q) * 128 + t], Fy + q * fy.fstride + fy.at(i, j + 1, k));
+                    if (convz) {
+                        cp_async8(&opnd[(20 + q) * 128 + t], Fz + q * fz.fstride + fz.at(i, j, k));
+                        cp_async8(&opnd[(25 + q) * 128 + t], Fz + q * fz.fstride + fz.at(i, j, k + 1));
+                    }
                 }
             }
-            if constexpr (H > 0) {
+            if constexpr (H > 0 && OPS) {
                 const long long e = ((long long)i * b.ny + j) * b.nz + k;
 #pragma unroll
                 for (int q = 0; q < 4; q++) cp_async8(&opnd[(30 + q) * 128 + t], V + q * vs + e);
@@ -287,12 +297,19 @@ __global__ void __launch_bounds__(128, 2)
         for (int q = 0; q < 5; q++) {
             r[q] += (f[q] - fprev[q * 128 + t]) * c.inv_dx;
             fprev[q * 128 + t] = f[q];
-            r[q] += (opnd[(15 + q) * 128 + t] - opnd[(10 + q) * 128 + t]) * c.inv_dy;
-            if (convz) r[q] += (opnd[(25 + q) * 128 + t] - opnd[(20 + q) * 128 + t]) * c.inv_dz;
+            if constexpr (OPS) {
+                r[q] += (opnd[(15 + q) * 128 + t] - opnd[(10 + q) * 128 + t]) * c.inv_dy;
+                if (convz) r[q] += (opnd[(25 + q) * 128 + t] - opnd[(20 + q) * 128 + t]) * c.inv_dz;
+            } else {
+                r[q] += (Fy[q * fy.fstride + fy.at(i, j + 1, k)] - Fy[q * fy.fstride + fy.at(i, j, k)]) * c.inv_dy;
+                if (convz)
+                    r[q] += (Fz[q * fz.fstride + fz.at(i, j, k + 1)] - Fz[q * fz.fstride + fz.at(i, j, k)]) * c.inv_dz;
+            }
         }
         if constexpr (H > 0) {
 #pragma unroll
-            for (int q = 1; q < 5; q++) r[q] += opnd[(29 + q) * 128 + t];
+            for (int q = 1; q < 5; q++)
+                r[q] += OPS ? opnd[(29 + q) * 128 + t] : V[(q - 1) * vs + ((long long)i * b.ny + j) * b.nz + k];
         }
         double un[5], w[5];
 #pragma unroll
@@ -413,7 +430,7 @@ static void tma_dispatch(bool chr, bool borges, bool phys, const WTmaMaps& m, co
 
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
 static void xt_launch(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s) {
-    constexpr size_t bytes = XTmaLayout<H>::bytes;
+    constexpr size_t bytes = XTmaLayout<H, CHAR>::bytes;
     auto kern = k_xface_update_tma<CHAR, BORGES, PHYS, H, LAST>;
     // the attribute is per device; a refusal surfaces as the launch's error
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
