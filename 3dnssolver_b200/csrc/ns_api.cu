@@ -270,7 +270,10 @@ static void prof_mark(ns_ctx* ctx, int cls) {
 #define NS_FACE_TMA 1
 #endif
 #ifndef NS_VISC_TMA_MAX_ORDER
-#define NS_VISC_TMA_MAX_ORDER 6  // CD orders whose physical viscous terms march over TMA planes
+#define NS_VISC_TMA_MAX_ORDER 6  // CD orders whose viscous terms march over TMA planes
+#endif
+#ifndef NS_VISC_TMA_REF
+#define NS_VISC_TMA_REF 1  // the reference semantics' viscous terms too
 #endif
 #ifndef NS_XUPD_TMA
 #define NS_XUPD_TMA 1
@@ -495,8 +498,8 @@ static ns_status do_step(ns_ctx* ctx) {
             a.V = (const double*)ctx->F[0];
             a.vs = ctx->fb[0].fstride;
             const nsb::WTmaMaps* m = tma_maps(ctx);
-            if (m && phys(ctx) && ctx->c.order <= NS_VISC_TMA_MAX_ORDER)
-                launch_viscous_tma(ctx->c.order / 2, *m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
+            if (m && ctx->c.order <= NS_VISC_TMA_MAX_ORDER && (phys(ctx) || NS_VISC_TMA_REF))
+                launch_viscous_tma(ctx->c.order / 2, phys(ctx), *m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
                                    ctx->fb[0].fstride, ctx->slot + 4, s);
             else
                 launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],

@@ -381,6 +381,67 @@ __device__ __forceinline__ void viscous_reference(const double* __restrict__ W, 
                                 TV(W[1 * fs + o]), TV(W[o]), c, r);
 }
 
+// Reference semantics: the terms of viscous_reference above, in the same
+// arithmetic order, from an accessor at(q, ox, oy) of W at offsets ox along x
+// and oy along y of the cell (the TMA-marched kernel reads its shared-memory
+// planes through it).  The mixed derivatives read the rows/columns the
+// per-thread kernel wraps to; the box holds them as the filled face halos.
+template <int H, typename TV, typename At>
+__device__ __forceinline__ void viscous_reference_core(At at, const Box& b, const Consts& c, int i, int j,
+                                                       TV r[5]) {
+    TV cx1[2 * H + 1], cy1[2 * H + 1], cxx[2 * H + 1], cyy[2 * H + 1];
+#pragma unroll
+    for (int t = 0; t <= 2 * H; t++) {
+        cx1[t] = TV(c.df[3 - H + t] * c.inv_dx);
+        cy1[t] = TV(c.df[3 - H + t] * c.inv_dy);
+        cxx[t] = TV(c.ddf[3 - H + t] * c.inv_dx * c.inv_dx);
+        cyy[t] = TV(c.ddf[3 - H + t] * c.inv_dy * c.inv_dy);
+    }
+    TV Dx[4], Dy[4], Dxx[4], Dyy[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        TV sx1 = 0, sy1 = 0, sxx = 0, syy = 0;
+#pragma unroll
+        for (int t = 0; t <= 2 * H; t++) {
+            TV wx = TV(at(q, t - H, 0));
+            TV wy = TV(at(q, 0, t - H));
+            if (t != H) { sx1 += wx * cx1[t]; sy1 += wy * cy1[t]; }
+            sxx += wx * cxx[t];
+            syy += wx * cyy[t];
+        }
+        Dx[q] = sx1; Dy[q] = sy1; Dxx[q] = sxx; Dyy[q] = syy;
+    }
+    TV Dxy[2], Dyx[2];
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+        const int q = 2 + v;
+        TV sxy = 0, syx = 0;
+#pragma unroll
+        for (int s = 0; s <= 2 * H; s++) {
+            if (s == H) continue;
+            const int jj = j + s - H;
+            {
+                TV dx = 0;
+#pragma unroll
+                for (int t = 0; t <= 2 * H; t++)
+                    if (t != H) dx += TV(at(q, t - H, s - H)) * cx1[t];
+                if ((jj >= 0 && jj < b.ny) || c.periodic[1]) sxy += dx * cy1[s];
+            }
+            const int ii = i + s - H;
+            {
+                TV dy = 0;
+#pragma unroll
+                for (int t = 0; t <= 2 * H; t++)
+                    if (t != H) dy += TV(at(q, s - H, t - H)) * cy1[t];
+                if (x_inside(ii, b.nx, c)) syx += dy * cx1[s];
+            }
+        }
+        Dxy[v] = sxy; Dyx[v] = syx;
+    }
+    viscous_reference_terms<TV>(Dx, Dy, Dxx, Dyy, Dxy, Dyx, TV(at(2, 0, 0)), TV(at(3, 0, 0)), TV(at(1, 0, 0)),
+                                TV(at(0, 0, 0)), c, r);
+}
+
 // Physical semantics: the full 3D viscous terms of viscous_physical below, in
 // the same arithmetic order, from two accessors of W around the cell (the
 // TMA-marched kernel reads its shared-memory planes through them; the
@@ -688,7 +749,7 @@ struct ViscRing {
     static constexpr int MINB = H == 1 ? 4 : (H == 2 ? 3 : 2);
 };
 
-template <int H>
+template <int H, bool PHYS>
 __global__ void __launch_bounds__(128, ViscRing<H>::MINB)
     k_viscous_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ W, Box b, Consts c,
                   double* __restrict__ V, long long vs, unsigned long long* __restrict__ err) {
@@ -735,7 +796,16 @@ __global__ void __launch_bounds__(128, ViscRing<H>::MINB)
         if (ok && live) {
             double rv[5] = {0, 0, 0, 0, 0};
             if (nbjk + (i < H || i >= b.nx - H) >= 2) {
-                viscous_physical<H, double>(W, b, c, i, j, k, rv);
+                if constexpr (PHYS)
+                    viscous_physical<H, double>(W, b, c, i, j, k, rv);
+                else
+                    viscous_reference<H, double>(W, b, c, i, j, k, rv);
+            } else if constexpr (!PHYS) {
+                const double* P[2 * H + 1];
+#pragma unroll
+                for (int s = 0; s <= 2 * H; s++) P[s] = vring + slot(i - H + s) * STRIDE;
+                auto at = [&](int q, int ox, int oy) { return P[H + ox][q * QS + cc + oy * BZ]; };
+                viscous_reference_core<H, double>(at, b, c, i, j, rv);
             } else {
                 const double* P[2 * H + 1];
 #pragma unroll
@@ -1248,22 +1318,28 @@ static void visc_one(const double* W, const Box& b, const Consts& c, double* V, 
     k_viscous<H, PHYS><<<interior_grid(b), dim3(32, 4), 0, s>>>(W, b, c, V, vs);
 }
 
-template <int H>
+template <int H, bool PHYS>
 static void visc_tma_one(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V, long long vs,
                          unsigned long long* err, cudaStream_t s) {
     constexpr size_t bytes = ViscRing<H>::smem;
     // the attribute is per device; a refusal surfaces as the launch's error
-    cudaFuncSetAttribute(k_viscous_tma<H>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(k_viscous_tma<H, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     const dim3 grid((b.nz + 31) / 32, (b.ny + 3) / 4, (b.nx + VISC_LX - 1) / VISC_LX);
-    k_viscous_tma<H><<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[3 + H - 1]), W, b,
-                                                       c, V, vs, err);
+    k_viscous_tma<H, PHYS><<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[3 + H - 1]),
+                                                             W, b, c, V, vs, err);
 }
 
-void launch_viscous_tma(int h, const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
+void launch_viscous_tma(int h, bool phys, const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
                         long long vs, unsigned long long* err, cudaStream_t s) {
-    if (h == 1) visc_tma_one<1>(m, W, b, c, V, vs, err, s);
-    else if (h == 2) visc_tma_one<2>(m, W, b, c, V, vs, err, s);
-    else visc_tma_one<3>(m, W, b, c, V, vs, err, s);
+    if (phys) {
+        if (h == 1) visc_tma_one<1, true>(m, W, b, c, V, vs, err, s);
+        else if (h == 2) visc_tma_one<2, true>(m, W, b, c, V, vs, err, s);
+        else visc_tma_one<3, true>(m, W, b, c, V, vs, err, s);
+    } else {
+        if (h == 1) visc_tma_one<1, false>(m, W, b, c, V, vs, err, s);
+        else if (h == 2) visc_tma_one<2, false>(m, W, b, c, V, vs, err, s);
+        else visc_tma_one<3, false>(m, W, b, c, V, vs, err, s);
+    }
 }
 
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,

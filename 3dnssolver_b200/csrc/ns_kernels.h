@@ -142,10 +142,10 @@ void launch_xface_update_tma(bool chr, bool borges, const UpdateArgs& a, const W
 // vs >= nx ny nz), half-width h = order/2 of the centered scheme
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
                     long long vs, cudaStream_t s);
-// the same for physical semantics from TMA-loaded planes of the W that m maps,
-// marched along x (half-width h = 1, 2, 3); *err receives 1 if a wait ran out
-void launch_viscous_tma(int h, const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
-                        long long vs, unsigned long long* err, cudaStream_t s);
+// the same from TMA-loaded planes of the W that m maps, marched along x
+// (half-width h = 1, 2, 3); *err receives 1 if a wait ran out
+void launch_viscous_tma(int h, bool phys, const WTmaMaps& m, const double* W, const Box& b, const Consts& c,
+                        double* V, long long vs, unsigned long long* err, cudaStream_t s);
 // slab halo exchange: pack the outer interior planes of a side / unpack into its ghost planes
 void launch_slab_pack(const double* U, const Box& b, int side, double* buf, cudaStream_t s);
 void launch_slab_unpack(double* U, const Box& b, int side, const double* buf, cudaStream_t s);
