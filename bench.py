@@ -279,20 +279,20 @@ COMPUTE_PER_UNIT = {
     ("reference", "fp64_char", "face_z"): (1395, 1003, "fp64", "face"),
     ("reference", "fp64_comp", "face_y"): (1041, 789, "fp64", "face"),
     ("reference", "fp64_comp", "face_z"): (1041, 789, "fp64", "face"),
-    ("reference", "fp64_char", "xface_update"): (1550, 1108, "fp64", "cell"),
-    ("reference", "fp64_comp", "xface_update"): (1161, 859, "fp64", "cell"),
-    ("reference", "fp64_char", "viscous"): (222, 136, "fp64", "cell"),
-    ("reference", "fp64_comp", "viscous"): (222, 136, "fp64", "cell"),
+    ("reference", "fp64_char", "xface_update"): (1528, 1092, "fp64", "cell"),
+    ("reference", "fp64_comp", "xface_update"): (1144, 846, "fp64", "cell"),
+    ("reference", "fp64_char", "viscous"): (221, 135, "fp64", "cell"),
+    ("reference", "fp64_comp", "viscous"): (221, 135, "fp64", "cell"),
     ("reference", "fp32_char", "stage_fused"): (4216, 2885, "fp32", "cell"),
     ("reference", "fp32_comp", "stage_fused"): (3211, 2244, "fp32", "cell"),
     ("physical", "fp64_char", "face_y"): (1441, 1032, "fp64", "face"),
     ("physical", "fp64_char", "face_z"): (1441, 1032, "fp64", "face"),
     ("physical", "fp64_comp", "face_y"): (1078, 802, "fp64", "face"),
     ("physical", "fp64_comp", "face_z"): (1078, 802, "fp64", "face"),
-    ("physical", "fp64_char", "xface_update"): (1614, 1149, "fp64", "cell"),
-    ("physical", "fp64_comp", "xface_update"): (1237, 909, "fp64", "cell"),
-    ("physical", "fp64_char", "viscous"): (369, 202, "fp64", "cell"),
-    ("physical", "fp64_comp", "viscous"): (369, 202, "fp64", "cell"),
+    ("physical", "fp64_char", "xface_update"): (1592, 1133, "fp64", "cell"),
+    ("physical", "fp64_comp", "xface_update"): (1219, 896, "fp64", "cell"),
+    ("physical", "fp64_char", "viscous"): (392, 225, "fp64", "cell"),
+    ("physical", "fp64_comp", "viscous"): (392, 225, "fp64", "cell"),
     ("physical", "fp32_char", "stage_fused"): (4486, 3070, "fp32", "cell"),
     ("physical", "fp32_comp", "stage_fused"): (3521, 2448, "fp32", "cell"),
 }
@@ -303,14 +303,14 @@ COMPUTE_PER_UNIT = {
 TRAFFIC_PER_UNIT = {
     ("reference", "fp64_char", "face_y"): 68.6, ("reference", "fp64_char", "face_z"): 65.7,
     ("reference", "fp64_comp", "face_y"): 66.0, ("reference", "fp64_comp", "face_z"): 63.2,
-    ("reference", "fp64_char", "xface_update"): 321.2, ("reference", "fp64_comp", "xface_update"): 320.7,
-    ("reference", "fp64_char", "viscous"): 51.2, ("reference", "fp64_comp", "viscous"): 51.2,
+    ("reference", "fp64_char", "xface_update"): 320.6, ("reference", "fp64_comp", "xface_update"): 317.9,
+    ("reference", "fp64_char", "viscous"): 61.8, ("reference", "fp64_comp", "viscous"): 61.7,
     ("reference", "fp64_char", "fill_prim"): 21.8, ("reference", "fp64_comp", "fill_prim"): 21.7,
     ("reference", "fp32_char", "stage_fused"): 119.2, ("reference", "fp32_comp", "stage_fused"): 119.4,
     ("physical", "fp64_char", "face_y"): 67.3, ("physical", "fp64_char", "face_z"): 65.3,
     ("physical", "fp64_comp", "face_y"): 65.1, ("physical", "fp64_comp", "face_z"): 62.5,
-    ("physical", "fp64_char", "xface_update"): 320.9, ("physical", "fp64_comp", "xface_update"): 320.7,
-    ("physical", "fp64_char", "viscous"): 61.6, ("physical", "fp64_comp", "viscous"): 61.7,
+    ("physical", "fp64_char", "xface_update"): 319.5, ("physical", "fp64_comp", "xface_update"): 318.0,
+    ("physical", "fp64_char", "viscous"): 61.8, ("physical", "fp64_comp", "viscous"): 61.8,
     ("physical", "fp64_char", "fill_prim"): 21.6, ("physical", "fp64_comp", "fill_prim"): 21.9,
     ("physical", "fp32_char", "stage_fused"): 118.9, ("physical", "fp32_comp", "stage_fused"): 119.0,
 }
@@ -362,7 +362,7 @@ def rooflines(form, prof, n, ms_per_step, peaks, fma, semantics):
     kname = KERNEL_NAMES.get(dom, dom)
     if sem == "physical" and dom in ("face_y", "face_z"):
         kname = kname.replace("k_face_flux", "k_face_flux_tma")
-    if sem == "physical" and dom == "viscous":
+    if dom == "viscous":
         kname = "k_viscous_tma<%d>" % (FORMS[form].get("order", 2) // 2)
     kname += f" ({form})"
     hbm = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
