@@ -7,6 +7,8 @@ to the reference by tests/test_oracle_golden.py).
             right-hand side and one time step
   config 3: Sod shock tube, characteristic-wise, one time step on 128x32x32 with
             the stable setting Ly = Lz = 1 (dy = dz = 4 dx at 512x128x128; here 4 dx too)
+  config 5: Taylor-Green vortex, physical semantics, characteristic-wise, 20 steps
+            at 64^3 (FP64 and FP32), and with CD-6 + Borges weights 5 steps at 48^3
 
 Tolerance: 1e-12 relative L2 per conserved field, as in tests/test_gpu_parity.py,
 for every state.  The 256^3 right-hand side alone is judged at 1e-11: at that
@@ -94,3 +96,46 @@ def test_config3_sod_characteristic_one_step(oracle):
     err_t = np.sqrt(((interior(Ug)[..., 3:5] - interior(Uo)[..., 3:5]) ** 2).sum((0, 1, 2))) / mag
     assert (err[:3] <= TOL).all(), f"config 3 one step: rel L2 per field {err}"
     assert (err_t <= TOL).all(), err_t
+
+
+def _tgv(n, **kw):
+    L = 2 * math.pi
+    args = dict(L=(L, L, L), mu=1.0 / 1600.0, Pr=0.72, cfl=0.5, convection=pkg.CONV_WENO5_CHAR,
+                diffusion_order=2, semantics=pkg.SEM_PHYSICAL)
+    args.update(kw)
+    return pkg.make_params(n, n, n, **args)
+
+
+def test_config5_taylor_green_physical_64_characteristic_20_steps(oracle):
+    """The headline workload's semantics, schemes and initial condition at 64^3 over
+    20 steps (TMA face tiles, x-march ring and viscous march over many blocks):
+    FP64 against the oracle at 1e-12, FP32 at FP32 accuracy."""
+    p = _tgv(64)
+    W0 = wl.taylor_green(p)
+    Wo, Uo, dto = oracle.run(p, W0, 20)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(20)
+        Ug = s.download_conservative()
+        dt, t = s.get_dt()
+    _check(Ug, Uo, "Taylor-Green 64^3 after 20 steps")
+    assert t == pytest.approx(dto.sum(), rel=1e-12)
+    with pkg.Solver(_tgv(64, precision=pkg.PREC_FP32)) as s:
+        s.upload_primitive(W0)
+        s.advance(20)
+        U32 = s.download_conservative()
+    err = rel_l2(interior(U32), interior(Uo))
+    assert (err[:2] <= 1e-6).all(), f"FP32 rel L2 per field {err}"
+
+
+def test_taylor_green_physical_cd6_borges_48_five_steps(oracle):
+    """CD-6 viscous terms and Borges weights at 48^3 (the TMA viscous march of
+    half-width 3) against the oracle."""
+    p = _tgv(48, diffusion_order=6, weights=pkg.WEIGHTS_BORGES)
+    W0 = wl.taylor_green(p)
+    Wo, Uo, dto = oracle.run(p, W0, 5)
+    with pkg.Solver(p) as s:
+        s.upload_primitive(W0)
+        s.advance(5)
+        Ug = s.download_conservative()
+    _check(Ug, Uo, "Taylor-Green 48^3 CD-6 Borges after 5 steps")
