@@ -52,10 +52,13 @@ namespace nsb {
 #ifndef NS_MARCH_TY
 #define NS_MARCH_TY 8
 #endif
-// cells a block marches along x
-#ifndef NS_MARCH_LX
-#define NS_MARCH_LX 32
-#endif
+// cells a block marches along x: 64 ran 2.2% faster than 32 for the
+// characteristic-wise stage on B200 at 256^3 and 0.5% slower for the
+// component-wise one
+template <bool CHAR>
+struct MarchLen {
+    static constexpr int value = CHAR ? 64 : 32;
+};
 //
 // Plane i reads planes i-2..i+3 (x-faces) and i-H..i+H (viscous terms).  With
 // H <= 1 ("lean") the ring holds 6 planes and the y/z face buffers alternate
@@ -72,7 +75,7 @@ namespace nsb {
 template <typename T, int H = 1>
 struct MarchTile {
     static_assert(sizeof(T) == 4, "the fused stage serves the FP32 form");
-    static constexpr int TY = NS_MARCH_TY, TZ = 32, LX = NS_MARCH_LX;
+    static constexpr int TY = NS_MARCH_TY, TZ = 32;
     static constexpr int FT = TY * TZ;  // threads per block, one per cell of the column
     static constexpr int PY = TY + 6, PZ = TZ + 6, NP = PY * PZ;
     static constexpr bool LEAN = H <= 1;
@@ -268,8 +271,9 @@ __global__ void __launch_bounds__(MarchTile<T, H>::FT, MarchTile<T, H>::MINB)
     T* FZb = FYb + M::NBUF * 5 * M::NFY;         // [NBUF][5][NFZ]
     double* S = reinterpret_cast<double*>(FZb + M::NBUF * 5 * M::NFZ);  // [5][NP] U_in of the plane in flight
     const int tid = threadIdx.x, ty = tid / M::TZ, tz = tid % M::TZ;
-    const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * M::LX;
-    const int x1 = min(x0 + M::LX, b.nx);
+    constexpr int LX = MarchLen<CHAR>::value;
+    const int k0 = blockIdx.x * M::TZ, j0 = blockIdx.y * M::TY, x0 = blockIdx.z * LX;
+    const int x1 = min(x0 + LX, b.nx);
     auto plane = [&](int i) { return ring + ring_slot<M::RING>(i, x0) * 5 * M::NP; };
     // U_in of plane i at folded positions, into S without waiting (each thread
     // later converts exactly the elements it copied, so S needs no barrier)
@@ -430,7 +434,8 @@ static cudaError_t fused_one(const FusedArgs& a, cudaStream_t s) {
     // the attribute is per device; setting it on every launch keeps multi-device use correct
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + M::LX - 1) / M::LX);
+    constexpr int LX = MarchLen<CHAR>::value;
+    dim3 grid((a.b.nz + M::TZ - 1) / M::TZ, (a.b.ny + M::TY - 1) / M::TY, (a.b.nx + LX - 1) / LX);
     kern<<<grid, M::FT, M::smem, s>>>(a.Uin, a.U0, a.Uout, a.b, a.c, a.conv_dims, a.m1, a.m2, a.mc, a.slot,
                                    a.slot_next, a.clock, a.skip);
     return cudaGetLastError();
