@@ -75,10 +75,16 @@ __device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma, T inv_gm1) {
     e.q2 = e.vel[0] * e.vel[0] + e.vel[1] * e.vel[1] + e.vel[2] * e.vel[2];
     T K = gamma - T(1);
     if constexpr (PHYS) {
-        e.c2 = gamma * p * trcp(rho);
-        e.c = tsqrt(e.c2);
-        e.Kpc = K * T(0.5) * trcp(e.c2);
-        e.inv2c = T(0.5) * trcp(e.c);
+        // c2 = gamma p / rho from one r = rsqrt(gamma p rho): c = gamma p r,
+        // 1/c = rho r, so no division or square root (each costs a Newton
+        // sequence in FP64)
+        const T gp = gamma * p;
+        const T r = trsqrt(gp * rho);
+        const T ic = rho * r;
+        e.c = gp * r;
+        e.c2 = e.c * e.c;
+        e.Kpc = K * T(0.5) * (ic * ic);
+        e.inv2c = T(0.5) * ic;
     } else {
         T pr = p * rho;
         T r = trsqrt(pr);
