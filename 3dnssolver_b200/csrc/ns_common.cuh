@@ -233,6 +233,27 @@ __device__ __forceinline__ void weno_right_nd(T a, T b, T c, T d, T e, T& num, T
     den = T(6) * (n0 + n1 + n2);
 }
 
+// x / d for a positive, normal d (the WENO denominators: sums of products of
+// squared smoothness indicators, each at least the epsilon): the reciprocal by
+// two Newton-Raphson iterations y <- y + y (1 - d y) from the hardware estimate
+// (PTX rcp.approx.ftz.f64), then the quotient with one Markstein correction
+// (P. Markstein, IA-64 and Elementary Functions, 2000): q = x y, r = x - d q,
+// q + r y.  Within an ulp of the rounded quotient.
+#ifndef NS_WENO_NR
+#define NS_WENO_NR 1
+#endif
+__device__ __forceinline__ double div_pos_nr(double x, double d) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-d, y, 1.0);
+    y = fma(y, e, y);
+    const double q = x * y;
+    const double r = fma(-d, q, x);
+    return fma(r, y, q);
+}
+
 // f = WENO5_left(l) + WENO5_right(r) with one division in FP64:
 // nL/dL + nR/dR = (nL dR + nR dL)/(dL dR); FP32 uses two fast reciprocals.
 template <typename T, bool BORGES>
@@ -240,8 +261,10 @@ __device__ __forceinline__ T weno_pair(T l0, T l1, T l2, T l3, T l4, T r0, T r1,
     T nL, dL, nR, dR;
     weno_left_nd<T, BORGES>(l0, l1, l2, l3, l4, nL, dL);
     weno_right_nd<T, BORGES>(r0, r1, r2, r3, r4, nR, dR);
-    if constexpr (sizeof(T) == 8)
-        return (nL * dR + nR * dL) / (dL * dR);
+    if constexpr (sizeof(T) == 8) {
+        if constexpr (NS_WENO_NR) return div_pos_nr(nL * dR + nR * dL, dL * dR);
+        else return (nL * dR + nR * dL) / (dL * dR);
+    }
     else
         return __fdividef(nL, dL) + __fdividef(nR, dR);
 }

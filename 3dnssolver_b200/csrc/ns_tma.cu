@@ -178,8 +178,11 @@ struct XTmaLayout {
     static constexpr size_t bytes = (size_t)(NSLOT * STRIDE + (5 + NOP) * 128) * 8 + NSLOT * 8;
 };
 
+// Two blocks per SM for the characteristic-wise march (255 registers, no
+// spills); three for the component-wise one (its 54 KB of shared memory allow
+// them, and 170 registers hold it).
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
-__global__ void __launch_bounds__(128, 2)
+__global__ void __launch_bounds__(128, CHAR ? 2 : 3)
     k_xface_update_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ U, double* __restrict__ U0,
                        double* __restrict__ Uout, double* __restrict__ Wn, const double* __restrict__ Fy,
                        const double* __restrict__ Fz, const double* __restrict__ V, long long vs, Box b, FaceBox fy,
