@@ -80,6 +80,7 @@ def load_library():
         "ns_set_sensor_weights": ([C, fp], st),
         "ns_fma_peak": ([ctypes.c_int, dp], st),
         "ns_wait_selftest": ([ctypes.c_uint, ctypes.POINTER(ctypes.c_int), dp], st),
+        "ns_div_selftest": ([ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong)], st),
         "ns_get_dt": ([C, dp, dp], st),
     }
     for name, (args, res) in protos.items():
@@ -138,6 +139,13 @@ def wait_selftest(polls=4096):
     r, t = ctypes.c_int(), ctypes.c_double()
     _check(load_library().ns_wait_selftest(int(polls), ctypes.byref(r), ctypes.byref(t)), "ns_wait_selftest")
     return bool(r.value), t.value
+
+
+def div_selftest(n=1 << 22, seed=7):
+    """Largest ulp distance of the FP64 WENO quotient from the IEEE quotient over n draws."""
+    m = ctypes.c_ulonglong()
+    _check(load_library().ns_div_selftest(int(n), int(seed), ctypes.byref(m)), "ns_div_selftest")
+    return m.value
 
 
 def sensor_init(seed):

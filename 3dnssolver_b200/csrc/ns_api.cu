@@ -957,6 +957,20 @@ ns_status ns_profile_step(ns_ctx* ctx, float* ms, int n) {
 
 long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+ns_status ns_div_selftest(long long n, unsigned long long seed, unsigned long long* max_ulp) {
+    if (!max_ulp || n <= 0) return fail(NS_ERR_INVALID_ARG, "max_ulp must be non-NULL and n positive");
+    unsigned long long* d = nullptr;
+    NS_CUDA(cudaMalloc(&d, sizeof *d));
+    ns_status st = NS_OK;
+    unsigned long long h = 0;
+    if (cudaMemset(d, 0, sizeof *d) != cudaSuccess || launch_div_check(n, seed, d, nullptr) != cudaSuccess ||
+        cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = fail(NS_ERR_CUDA, "division self-test failed: %s", cudaGetErrorString(cudaGetLastError()));
+    cudaFree(d);
+    if (st == NS_OK) *max_ulp = h;
+    return st;
+}
+
 ns_status ns_wait_selftest(unsigned polls, int* ran_out, double* ms) {
     if (!ran_out || !ms) return fail(NS_ERR_INVALID_ARG, "ran_out and ms must be non-NULL");
     if (polls == 0 || polls > (1u << 24)) return fail(NS_ERR_INVALID_ARG, "polls must lie in 1 .. 2^24");

@@ -987,6 +987,36 @@ __global__ void __launch_bounds__(128, XupdMinBlocks<CHAR, PHYS>::value)
 }
 
 // ---------------------------------------------------------------------------
+// error bound of div_pos_nr against the IEEE quotient: n quotients x / d with x
+// log-uniform in [1e-3, 1e3] and d log-uniform in [1e-60, 1e60] (SplitMix64
+// draws); *max_ulp receives the largest distance in units in the last place
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__global__ void k_div_check(long long n, unsigned long long seed, unsigned long long* __restrict__ max_ulp) {
+    unsigned long long worst = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double u = (splitmix64(seed + 2 * e) >> 11) * 0x1.0p-53;
+        const double v = (splitmix64(seed + 2 * e + 1) >> 11) * 0x1.0p-53;
+        const double x = exp10(-3.0 + 6.0 * u), d = exp10(-60.0 + 120.0 * v);
+        const long long a = __double_as_longlong(div_pos_nr(x, d)), b = __double_as_longlong(x / d);
+        const unsigned long long dist = (unsigned long long)(a > b ? a - b : b - a);
+        if (dist > worst) worst = dist;
+    }
+    atomicMax(max_ulp, worst);
+}
+
+cudaError_t launch_div_check(long long n, unsigned long long seed, unsigned long long* max_ulp, cudaStream_t s) {
+    k_div_check<<<256, 256, 0, s>>>(n, seed, max_ulp);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // host <-> device layout transposes (reference AoS [i][j][k][q], unpadded
 // (nx+6)(ny+6)(nz+6) x 5  <->  device SoA planes)
 

@@ -128,6 +128,8 @@ bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b);
 void launch_face_flux_tma(int dir, bool chr, bool borges, bool phys, const WTmaMaps& m, const double* W,
                           const Box& b, const Consts& c, void* F, const FaceBox& fb, int sms,
                           unsigned long long* err, cudaStream_t s);
+// largest ulp distance between div_pos_nr and the IEEE quotient over n draws
+cudaError_t launch_div_check(long long n, unsigned long long seed, unsigned long long* max_ulp, cudaStream_t s);
 // one block waits (bounded) on an mbarrier phase nothing completes; out[0] = 1
 // if the wait gave up, 0 if it claimed completion
 cudaError_t launch_wait_probe(unsigned polls, unsigned long long* out, cudaStream_t s);

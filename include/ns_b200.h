@@ -310,6 +310,11 @@ NS_API ns_status ns_fma_peak(int fp64, double* tflops);
  * device stays usable afterwards (no fault, no trap).  No reference
  * counterpart. */
 NS_API ns_status ns_wait_selftest(unsigned polls, int* ran_out, double* ms);
+/* Self-test of the FP64 WENO quotient (Newton-Raphson reciprocal from the
+ * hardware estimate with a Markstein correction) against the IEEE quotient on
+ * `n` seeded random pairs: *max_ulp = the largest distance in units in the
+ * last place.  No reference counterpart. */
+NS_API ns_status ns_div_selftest(long long n, unsigned long long seed, unsigned long long* max_ulp);
 /* Device kernels launched by this context since creation (for launch accounting). */
 NS_API long long ns_kernel_launches(ns_ctx* ctx);
 

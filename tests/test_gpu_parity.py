@@ -301,3 +301,10 @@ def test_taylor_green_physical_fp64_and_fp32_match_the_oracle(oracle):
         U32 = s.download_conservative()
     err = rel_l2(interior(U32), interior(Uo))
     assert (err[[0, 1]] <= 1e-6).all(), err
+
+
+def test_weno_quotient_within_one_ulp_of_ieee_division():
+    """The FP64 WENO weights divide by Newton-Raphson from the hardware reciprocal
+    estimate with a Markstein correction; over 4 M seeded pairs spanning 120
+    decades it stays within one unit in the last place of the IEEE quotient."""
+    assert pkg.div_selftest(1 << 22, seed=7) <= 1
