@@ -443,7 +443,8 @@ __device__ __forceinline__ void viscous_reference_core(At at, const Box& b, cons
 }
 
 // Physical semantics: the full 3D viscous terms of viscous_physical below, in
-// the same arithmetic order, from two accessors of W around the cell (the
+// the same arithmetic order (p / rho by div_pos_nr, within an ulp of the
+// division), from two accessors of W around the cell (the
 // TMA-marched kernel reads its shared-memory planes through them; the
 // per-thread kernel keeps its own loads, which compile to fewer registers):
 // ld1(q, ax, t) = field q at offset t - H along axis ax, ld2(q, a, s, bx, t) =
@@ -475,7 +476,10 @@ __device__ __forceinline__ void viscous_physical_core(Ld1 ld1, Ld2 ld2, const Co
         if (bx == 2 && !three) continue;
 #pragma unroll
         for (int t = 0; t < NS; t++) {
-            const TV T = TV(ld1(1, bx, t)) / TV(ld1(0, bx, t));
+            // p / rho (rho > 0): the Newton-Raphson quotient of the WENO weights in FP64
+            TV T;
+            if constexpr (sizeof(TV) == 8) T = div_pos_nr(ld1(1, bx, t), ld1(0, bx, t));
+            else T = TV(ld1(1, bx, t)) / TV(ld1(0, bx, t));
 #pragma unroll
             for (int a = 0; a < 3; a++) {
                 const TV va = TV(ld1(2 + a, bx, t));
