@@ -142,10 +142,11 @@ def wait_selftest(polls=4096):
 
 
 def div_selftest(n=1 << 22, seed=7):
-    """Largest ulp distance of the FP64 WENO quotient from the IEEE quotient over n draws."""
-    m = ctypes.c_ulonglong()
-    _check(load_library().ns_div_selftest(int(n), int(seed), ctypes.byref(m)), "ns_div_selftest")
-    return m.value
+    """Largest ulp distances over n draws: (WENO quotient vs IEEE division,
+    Newton-Raphson 1/sqrt vs CUDA's rsqrt)."""
+    m = (ctypes.c_ulonglong * 2)()
+    _check(load_library().ns_div_selftest(int(n), int(seed), m), "ns_div_selftest")
+    return int(m[0]), int(m[1])
 
 
 def sensor_init(seed):

@@ -960,14 +960,17 @@ long long ns_kernel_launches(ns_ctx* ctx) { return ctx ? ctx->launches : 0; }
 ns_status ns_div_selftest(long long n, unsigned long long seed, unsigned long long* max_ulp) {
     if (!max_ulp || n <= 0) return fail(NS_ERR_INVALID_ARG, "max_ulp must be non-NULL and n positive");
     unsigned long long* d = nullptr;
-    NS_CUDA(cudaMalloc(&d, sizeof *d));
+    NS_CUDA(cudaMalloc(&d, 2 * sizeof *d));
     ns_status st = NS_OK;
-    unsigned long long h = 0;
-    if (cudaMemset(d, 0, sizeof *d) != cudaSuccess || launch_div_check(n, seed, d, nullptr) != cudaSuccess ||
-        cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
+    unsigned long long h[2] = {0, 0};
+    if (cudaMemset(d, 0, 2 * sizeof *d) != cudaSuccess || launch_div_check(n, seed, d, nullptr) != cudaSuccess ||
+        cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess)
         st = fail(NS_ERR_CUDA, "division self-test failed: %s", cudaGetErrorString(cudaGetLastError()));
     cudaFree(d);
-    if (st == NS_OK) *max_ulp = h;
+    if (st == NS_OK) {
+        max_ulp[0] = h[0];
+        max_ulp[1] = h[1];
+    }
     return st;
 }
 

@@ -254,6 +254,21 @@ __device__ __forceinline__ double div_pos_nr(double x, double d) {
     return fma(r, y, q);
 }
 
+// 1 / sqrt(x) for a positive, normal x: two Newton-Raphson iterations
+// y <- y + (y / 2)(1 - x y^2) from the hardware estimate (PTX
+// rsqrt.approx.ftz.f64).  Within an ulp or two of the rounded value.
+#ifndef NS_RSQRT_NR
+#define NS_RSQRT_NR 1
+#endif
+__device__ __forceinline__ double rsqrt_pos_nr(double x) {
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x * y, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    e = fma(-x * y, y, 1.0);
+    return fma(0.5 * y, e, y);
+}
+
 // f = WENO5_left(l) + WENO5_right(r) with one division in FP64:
 // nL/dL + nR/dR = (nL dR + nR dL)/(dL dR); FP32 uses two fast reciprocals.
 template <typename T, bool BORGES>

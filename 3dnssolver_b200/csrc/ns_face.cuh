@@ -56,9 +56,15 @@ struct Eig {
     T vel[3], qn, ql, qm, q2, c, c2, H, Kpc, K2pc, inv2c;
 };
 
+// 1/sqrt(x), x > 0 (sound speeds): Newton-Raphson in FP64 (rsqrt_pos_nr)
 template <typename T>
 __device__ __forceinline__ T trsqrt(T x) {
-    if constexpr (sizeof(T) == 8) return rsqrt(x); else return rsqrtf(x);
+    if constexpr (sizeof(T) == 8) {
+        if constexpr (NS_RSQRT_NR) return rsqrt_pos_nr(x);
+        else return rsqrt(x);
+    } else {
+        return rsqrtf(x);
+    }
 }
 
 // Reference semantics (c2 = gamma/(p rho), convection_flux.cpp:139): one

@@ -991,9 +991,10 @@ __global__ void __launch_bounds__(128, XupdMinBlocks<CHAR, PHYS>::value)
 }
 
 // ---------------------------------------------------------------------------
-// error bound of div_pos_nr against the IEEE quotient: n quotients x / d with x
-// log-uniform in [1e-3, 1e3] and d log-uniform in [1e-60, 1e60] (SplitMix64
-// draws); *max_ulp receives the largest distance in units in the last place
+// error bounds of div_pos_nr against the IEEE quotient and of rsqrt_pos_nr
+// against CUDA's rsqrt: n pairs with x log-uniform in [1e-3, 1e3] and d
+// log-uniform in [1e-60, 1e60] (SplitMix64 draws); max_ulp[0], max_ulp[1]
+// receive the largest distances in units in the last place
 
 __device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
     z += 0x9E3779B97F4A7C15ull;
@@ -1003,7 +1004,7 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
 }
 
 __global__ void k_div_check(long long n, unsigned long long seed, unsigned long long* __restrict__ max_ulp) {
-    unsigned long long worst = 0;
+    unsigned long long worst = 0, worst_r = 0;
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const double u = (splitmix64(seed + 2 * e) >> 11) * 0x1.0p-53;
         const double v = (splitmix64(seed + 2 * e + 1) >> 11) * 0x1.0p-53;
@@ -1011,8 +1012,13 @@ __global__ void k_div_check(long long n, unsigned long long seed, unsigned long 
         const long long a = __double_as_longlong(div_pos_nr(x, d)), b = __double_as_longlong(x / d);
         const unsigned long long dist = (unsigned long long)(a > b ? a - b : b - a);
         if (dist > worst) worst = dist;
+        // 1/sqrt(d) against CUDA's rsqrt (itself within an ulp)
+        const long long ra = __double_as_longlong(rsqrt_pos_nr(d)), rb = __double_as_longlong(rsqrt(d));
+        const unsigned long long rdist = (unsigned long long)(ra > rb ? ra - rb : rb - ra);
+        if (rdist > worst_r) worst_r = rdist;
     }
     atomicMax(max_ulp, worst);
+    atomicMax(max_ulp + 1, worst_r);
 }
 
 cudaError_t launch_div_check(long long n, unsigned long long seed, unsigned long long* max_ulp, cudaStream_t s) {

@@ -310,10 +310,12 @@ NS_API ns_status ns_fma_peak(int fp64, double* tflops);
  * device stays usable afterwards (no fault, no trap).  No reference
  * counterpart. */
 NS_API ns_status ns_wait_selftest(unsigned polls, int* ran_out, double* ms);
-/* Self-test of the FP64 WENO quotient (Newton-Raphson reciprocal from the
- * hardware estimate with a Markstein correction) against the IEEE quotient on
- * `n` seeded random pairs: *max_ulp = the largest distance in units in the
- * last place.  No reference counterpart. */
+/* Self-test of the FP64 arithmetic written out in the kernels on `n` seeded
+ * random pairs: max_ulp[0] = the largest distance, in units in the last place,
+ * of the WENO quotient (Newton-Raphson reciprocal from the hardware estimate
+ * with a Markstein correction) from the IEEE quotient; max_ulp[1] = that of
+ * the sound-speed 1/sqrt (Newton-Raphson) from CUDA's rsqrt.  max_ulp points
+ * to two values.  No reference counterpart. */
 NS_API ns_status ns_div_selftest(long long n, unsigned long long seed, unsigned long long* max_ulp);
 /* Device kernels launched by this context since creation (for launch accounting). */
 NS_API long long ns_kernel_launches(ns_ctx* ctx);

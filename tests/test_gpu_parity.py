@@ -307,4 +307,6 @@ def test_weno_quotient_within_one_ulp_of_ieee_division():
     """The FP64 WENO weights divide by Newton-Raphson from the hardware reciprocal
     estimate with a Markstein correction; over 4 M seeded pairs spanning 120
     decades it stays within one unit in the last place of the IEEE quotient."""
-    assert pkg.div_selftest(1 << 22, seed=7) <= 1
+    q, r = pkg.div_selftest(1 << 22, seed=7)
+    assert q <= 1, q
+    assert r <= 2, r  # the sound-speed 1/sqrt against CUDA's rsqrt (each within an ulp)
