@@ -68,8 +68,9 @@ __device__ __forceinline__ T trsqrt(T x) {
 }
 
 // Reference semantics (c2 = gamma/(p rho), convection_flux.cpp:139): one
-// r = rsqrt(p rho) gives c = sqrt(gamma) r, 1/(2c) = p rho r / (2 sqrt(gamma))
-// and K/(2 c2) = (gamma-1) p rho / (2 gamma) without a division.
+// r = rsqrt(p rho) and one rg = rsqrt(gamma) give c = sqrt(gamma) r,
+// 1/(2c) = p rho r rg / 2 and K/(2 c2) = (gamma-1) p rho rg^2 / 2 without a
+// division or square root.
 template <int DIR, bool PHYS, typename T>
 __device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma, T inv_gm1) {
     Eig<T> e;
@@ -94,11 +95,13 @@ __device__ __forceinline__ Eig<T> make_eig(const T wa[5], T gamma, T inv_gm1) {
     } else {
         T pr = p * rho;
         T r = trsqrt(pr);
-        T sg = tsqrt(gamma);  // uniform across the warp; folded by the compiler per launch
-        e.c = sg * r;
+        // sqrt(gamma) and 1/gamma from one rg = rsqrt(gamma): no square root or
+        // division per face
+        const T rg = trsqrt(gamma);
+        e.c = (gamma * rg) * r;
         e.c2 = gamma * (r * r);
-        e.Kpc = (K * T(0.5) / gamma) * pr;
-        e.inv2c = (T(0.5) / sg) * (pr * r);
+        e.Kpc = (K * T(0.5) * (rg * rg)) * pr;
+        e.inv2c = (T(0.5) * rg) * (pr * r);
     }
     e.H = e.c2 * inv_gm1 + T(0.5) * e.q2;
     e.K2pc = T(2) * e.Kpc;  // K/c2
