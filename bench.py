@@ -275,25 +275,25 @@ def job_rate(world, cells, steps, ms_max):
 # vortex.  The x-update and fused stage rows average the three stages (the
 # third also forms the next step's start).
 COMPUTE_PER_UNIT = {
-    ("reference", "fp64_char", "face_y"): (1395, 1003, "fp64", "face"),
-    ("reference", "fp64_char", "face_z"): (1395, 1003, "fp64", "face"),
-    ("reference", "fp64_comp", "face_y"): (1041, 789, "fp64", "face"),
-    ("reference", "fp64_comp", "face_z"): (1041, 789, "fp64", "face"),
-    ("reference", "fp64_char", "xface_update"): (1528, 1092, "fp64", "cell"),
-    ("reference", "fp64_comp", "xface_update"): (1144, 846, "fp64", "cell"),
+    ("reference", "fp64_char", "face_y"): (1408, 996, "fp64", "face"),
+    ("reference", "fp64_char", "face_z"): (1406, 994, "fp64", "face"),
+    ("reference", "fp64_comp", "face_y"): (995, 748, "fp64", "face"),
+    ("reference", "fp64_comp", "face_z"): (995, 748, "fp64", "face"),
+    ("reference", "fp64_char", "xface_update"): (1533, 1079, "fp64", "cell"),
+    ("reference", "fp64_comp", "xface_update"): (1134, 841, "fp64", "cell"),
     ("reference", "fp64_char", "viscous"): (221, 135, "fp64", "cell"),
     ("reference", "fp64_comp", "viscous"): (221, 135, "fp64", "cell"),
     ("reference", "fp32_char", "stage_fused"): (4216, 2885, "fp32", "cell"),
     ("reference", "fp32_comp", "stage_fused"): (3211, 2244, "fp32", "cell"),
-    ("physical", "fp64_char", "face_y"): (1441, 1032, "fp64", "face"),
-    ("physical", "fp64_char", "face_z"): (1441, 1032, "fp64", "face"),
-    ("physical", "fp64_comp", "face_y"): (1078, 802, "fp64", "face"),
-    ("physical", "fp64_comp", "face_z"): (1078, 802, "fp64", "face"),
-    ("physical", "fp64_char", "xface_update"): (1592, 1133, "fp64", "cell"),
-    ("physical", "fp64_comp", "xface_update"): (1219, 896, "fp64", "cell"),
-    ("physical", "fp64_char", "viscous"): (392, 225, "fp64", "cell"),
-    ("physical", "fp64_comp", "viscous"): (392, 225, "fp64", "cell"),
-    ("physical", "fp32_char", "stage_fused"): (4486, 3070, "fp32", "cell"),
+    ("physical", "fp64_char", "face_y"): (1438, 1022, "fp64", "face"),
+    ("physical", "fp64_char", "face_z"): (1438, 1022, "fp64", "face"),
+    ("physical", "fp64_comp", "face_y"): (1091, 815, "fp64", "face"),
+    ("physical", "fp64_comp", "face_z"): (1091, 815, "fp64", "face"),
+    ("physical", "fp64_char", "xface_update"): (1590, 1123, "fp64", "cell"),
+    ("physical", "fp64_comp", "xface_update"): (1233, 909, "fp64", "cell"),
+    ("physical", "fp64_char", "viscous"): (378, 218, "fp64", "cell"),
+    ("physical", "fp64_comp", "viscous"): (378, 218, "fp64", "cell"),
+    ("physical", "fp32_char", "stage_fused"): (4440, 3037, "fp32", "cell"),
     ("physical", "fp32_comp", "stage_fused"): (3521, 2448, "fp32", "cell"),
 }
 # DRAM bytes (read + write) per unit from the same captures at 128^3 (inputs
@@ -301,16 +301,16 @@ COMPUTE_PER_UNIT = {
 # traffic scales with the units), averaged over the three stages of a step
 # like the counts above; "fill" is the steady-state k_fill_halo.
 TRAFFIC_PER_UNIT = {
-    ("reference", "fp64_char", "face_y"): 68.6, ("reference", "fp64_char", "face_z"): 65.7,
-    ("reference", "fp64_comp", "face_y"): 66.0, ("reference", "fp64_comp", "face_z"): 63.2,
-    ("reference", "fp64_char", "xface_update"): 320.6, ("reference", "fp64_comp", "xface_update"): 317.9,
-    ("reference", "fp64_char", "viscous"): 61.8, ("reference", "fp64_comp", "viscous"): 61.7,
+    ("reference", "fp64_char", "face_y"): 69.6, ("reference", "fp64_char", "face_z"): 63.5,
+    ("reference", "fp64_comp", "face_y"): 66.3, ("reference", "fp64_comp", "face_z"): 63.4,
+    ("reference", "fp64_char", "xface_update"): 319.9, ("reference", "fp64_comp", "xface_update"): 317.7,
+    ("reference", "fp64_char", "viscous"): 61.6, ("reference", "fp64_comp", "viscous"): 61.7,
     ("reference", "fp64_char", "fill_prim"): 21.8, ("reference", "fp64_comp", "fill_prim"): 21.7,
     ("reference", "fp32_char", "stage_fused"): 119.2, ("reference", "fp32_comp", "stage_fused"): 119.4,
-    ("physical", "fp64_char", "face_y"): 67.3, ("physical", "fp64_char", "face_z"): 65.3,
-    ("physical", "fp64_comp", "face_y"): 65.1, ("physical", "fp64_comp", "face_z"): 62.5,
-    ("physical", "fp64_char", "xface_update"): 319.5, ("physical", "fp64_comp", "xface_update"): 318.0,
-    ("physical", "fp64_char", "viscous"): 61.8, ("physical", "fp64_comp", "viscous"): 61.8,
+    ("physical", "fp64_char", "face_y"): 66.3, ("physical", "fp64_char", "face_z"): 62.9,
+    ("physical", "fp64_comp", "face_y"): 65.9, ("physical", "fp64_comp", "face_z"): 62.7,
+    ("physical", "fp64_char", "xface_update"): 319.6, ("physical", "fp64_comp", "xface_update"): 317.9,
+    ("physical", "fp64_char", "viscous"): 61.9, ("physical", "fp64_comp", "viscous"): 61.9,
     ("physical", "fp64_char", "fill_prim"): 21.6, ("physical", "fp64_comp", "fill_prim"): 21.9,
     ("physical", "fp32_char", "stage_fused"): 118.9, ("physical", "fp32_comp", "stage_fused"): 119.0,
 }
