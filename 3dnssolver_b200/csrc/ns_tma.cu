@@ -1,6 +1,7 @@
-// ns_tma.cu -- y- and z-face fluxes of the FP64 time steps from shared-memory
-// tiles that the Tensor Memory Accelerator (TMA) loads, and the tensor maps of
-// W that this kernel and the TMA-marched viscous kernel (ns_kernels.cu) use.
+// ns_tma.cu -- the FP64 time step's kernels that read W through the Tensor
+// Memory Accelerator (TMA): the y- and z-face fluxes from shared-memory tiles,
+// the x-march over a ring of planes, and the tensor maps of W that these and
+// the TMA-marched viscous kernel (ns_kernels.cu) use.
 //
 // The stencils of a time step read W only (U = cons(W) in registers).  A block
 // of 128 threads owns 4 face rows along y x 32 faces along z of one x-plane
@@ -156,9 +157,8 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
 // x-face between cells i and i+1 while plane i+4 is in flight; after the face
 // the block's threads release plane i-2 together (one block barrier) and
 // plane i+5 takes its slot.  The cell update's operands (U0, U, the y- and
-// z-face fluxes, the viscous terms) still come per thread with cp.async, and
-// the update itself is k_xface_update's.  Two blocks per SM, so the
-// characteristic-wise face keeps its registers without spilling.
+// z-face fluxes, the viscous terms) come per thread (below), and the update
+// itself is k_xface_update's.
 #ifndef NS_XT_LX
 #define NS_XT_LX 64
 #endif
