@@ -6,9 +6,11 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <utility>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "ns_common.cuh"
 #include "ns_kernels.h"
@@ -85,6 +87,9 @@ struct ns_ctx {
     bool flags_valid = false;                // the sensor's flags belong to the current state's run
     int sms = 148;                           // multiprocessors of the context's device
     nsb::WTmaMaps tma[2];                    // FP64 steps: tensor maps of W and W2 (face tiles, viscous planes)
+    // ns_time_step's transfer pipeline: the copy stream and its events (lazy)
+    cudaStream_t copy = nullptr;
+    std::vector<cudaEvent_t> ev;
 };
 
 static size_t host_elems(const ns_params* p) {
@@ -288,8 +293,10 @@ static const nsb::WTmaMaps* tma_maps(const ns_ctx* ctx) {
 }
 
 // face fluxes of the current (W, U) along every convected axis from first_dir on
-// (U: the context's, or the stage input Uin)
-static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullptr, bool w_only = false) {
+// (U: the context's, or the stage input Uin); pl: the x-planes of the y- and
+// z-faces of an FP64 time step (w_only), all planes by default
+static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullptr, bool w_only = false,
+                       Planes pl = Planes()) {
     const ns_params& p = ctx->p;
     const double* U = Uin ? Uin : ctx->U;
     if (p.convection == NS_CONV_NONE) return NS_OK;
@@ -310,11 +317,11 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullp
             if (m)
                 launch_face_flux_tma(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
                                      phys(ctx), *m, ctx->W, ctx->box, ctx->c, ctx->F[d], ctx->fb[d], ctx->sms,
-                                     ctx->slot + 4, ctx->stream);
+                                     ctx->slot + 4, ctx->stream, pl);
             else
                 launch_face_flux(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
                                  phys(ctx), fp32(ctx), ctx->W, U, ctx->box, ctx->c, ctx->F[d],
-                                 ctx->fb[d], ctx->stream, w_only);
+                                 ctx->fb[d], ctx->stream, w_only, w_only ? pl : Planes());
             NS_TRY(check_launch(ctx, d > 0 ? 2 : 1));  // y and z: the face grid and its last plane
         }
         prof_mark(ctx, NS_PROF_FACE_X + d);
@@ -426,14 +433,71 @@ static ns_status do_step_fused(ns_ctx* ctx) {
     return NS_OK;
 }
 
+// SSP-RK3 coefficients (time_scheme.cpp:36-38, 48-50, 60-62): U = U0 m1 + U m2 + R (mc dt)
+static const double kRkM1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
+static const double kRkM2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
+static const double kRkMc[3] = {-1.0, -(1. / 4.), -(2. / 3.)};
+
+// FP64 stage st after its fill, on the x-planes pl: the y- and z-faces (with
+// faces), the viscous terms, then the x-faces marched together with the cell
+// update from Uin into Uout (and the next stage's W into W2)
+static ns_status xstage(ns_ctx* ctx, int st, double* Uin, double* Uout, unsigned long long* cur,
+                        unsigned long long* nxt, bool with_faces, Planes pl) {
+    cudaStream_t s = ctx->stream;
+    if (with_faces) NS_TRY(faces(ctx, 1, Uin, true, pl));  // W = prim(U) here: the stencils read W only
+    UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
+    if (a.viscous) {  // into the x-face array, which the x-march leaves unused
+        a.V = (const double*)ctx->F[0];
+        a.vs = ctx->fb[0].fstride;
+        const nsb::WTmaMaps* m = tma_maps(ctx);
+        if (m && ctx->c.order <= NS_VISC_TMA_MAX_ORDER && (phys(ctx) || NS_VISC_TMA_REF))
+            launch_viscous_tma(ctx->c.order / 2, phys(ctx), *m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
+                               ctx->fb[0].fstride, ctx->slot + 4, s, pl);
+        else if (pl.n < 0)
+            launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
+                           ctx->fb[0].fstride, s);
+        else
+            return fail(NS_ERR_UNSUPPORTED, "a plane range of the viscous terms needs their TMA kernel");
+        NS_TRY(check_launch(ctx, 1));
+        prof_mark(ctx, NS_PROF_VISCOUS);
+    }
+    a.U = Uin;
+    a.Unext = Uout;
+    a.Wnext = ctx->W2;
+    a.slot = cur;
+    a.slot_next = (st == 2) ? nxt : nullptr;
+    a.m1 = kRkM1[st];
+    a.m2 = kRkM2[st];
+    a.mc = kRkMc[st];
+    a.clock = (st == 0) ? ctx->clock : nullptr;
+    const nsb::WTmaMaps* xm = NS_XUPD_TMA ? tma_maps(ctx) : nullptr;
+    if (xm)
+        launch_xface_update_tma(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, *xm,
+                                ctx->slot + 4, s, pl);
+    else if (pl.n < 0)
+        launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
+    else
+        return fail(NS_ERR_UNSUPPORTED, "a plane range of the x-march needs its TMA kernel");
+    NS_TRY(check_launch(ctx, 1));
+    prof_mark(ctx, NS_PROF_XFACE_UPDATE);
+    return NS_OK;
+}
+
+// the state after an FP64 step of do_step: U holds it, U0 and the other parity
+// slot the next step's start, W (after the last swap) the next stage's W
+static void end_xstep(ns_ctx* ctx) {
+    ctx->parity ^= 1;
+    ctx->fused_ready = true;
+    ctx->w_next_ready = true;
+    ctx->u_valid = true;
+    ctx->w_valid = false;
+    ctx->steps++;
+}
+
 // one TimeScheme::step on the device state
 static ns_status do_step(ns_ctx* ctx) {
     if (ctx->fused) return do_step_fused(ctx);
     cudaStream_t s = ctx->stream;
-    // SSP-RK3 coefficients (time_scheme.cpp:36-38, 48-50, 60-62)
-    const double m1[3] = {1.0, 3.0 / 4.0, 1. / 3.};
-    const double m2[3] = {0.0, 1.0 / 4.0, 2. / 3.};
-    const double mc[3] = {-1.0, -(1. / 4.), -(2. / 3.)};
     unsigned long long* cur = ctx->slot + ctx->parity;
     if (!ctx->xfused) {
         NS_CUDA(cudaMemsetAsync(cur, 0xFF, sizeof(unsigned long long), s));
@@ -449,9 +513,9 @@ static ns_status do_step(ns_ctx* ctx) {
             NS_TRY(faces(ctx));
             UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
             a.slot = cur;
-            a.m1 = m1[st];
-            a.m2 = m2[st];
-            a.mc = mc[st];
+            a.m1 = kRkM1[st];
+            a.m2 = kRkM2[st];
+            a.mc = kRkMc[st];
             a.clock = (st == 0) ? ctx->clock : nullptr;
             launch_update(a, s);
             NS_TRY(check_launch(ctx, 1));
@@ -492,46 +556,10 @@ static ns_status do_step(ns_ctx* ctx) {
             launch_fill_halo(ctx->W, in[st], ctx->box, ctx->c, s, out[st]);
         NS_TRY(check_launch(ctx, 1));
         prof_mark(ctx, NS_PROF_FILL);
-        NS_TRY(faces(ctx, 1, in[st], true));  // W = prim(U) here: the stencils read W only
-        UpdateArgs a = update_args(ctx, MODE_STAGE, true, true);
-        if (a.viscous) {  // into the x-face array, which the x-march leaves unused
-            a.V = (const double*)ctx->F[0];
-            a.vs = ctx->fb[0].fstride;
-            const nsb::WTmaMaps* m = tma_maps(ctx);
-            if (m && ctx->c.order <= NS_VISC_TMA_MAX_ORDER && (phys(ctx) || NS_VISC_TMA_REF))
-                launch_viscous_tma(ctx->c.order / 2, phys(ctx), *m, ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
-                                   ctx->fb[0].fstride, ctx->slot + 4, s);
-            else
-                launch_viscous(ctx->c.order / 2, phys(ctx), ctx->W, ctx->box, ctx->c, (double*)ctx->F[0],
-                               ctx->fb[0].fstride, s);
-            NS_TRY(check_launch(ctx, 1));
-            prof_mark(ctx, NS_PROF_VISCOUS);
-        }
-        a.U = in[st];
-        a.Unext = out[st];
-        a.Wnext = ctx->W2;
-        a.slot = cur;
-        a.slot_next = (st == 2) ? nxt : nullptr;
-        a.m1 = m1[st];
-        a.m2 = m2[st];
-        a.mc = mc[st];
-        a.clock = (st == 0) ? ctx->clock : nullptr;
-        const nsb::WTmaMaps* xm = NS_XUPD_TMA ? tma_maps(ctx) : nullptr;
-        if (xm)
-            launch_xface_update_tma(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a,
-                                    *xm, ctx->slot + 4, s);
-        else
-            launch_xface_update(ctx->p.convection == NS_CONV_WENO5_CHAR, ctx->p.weights == NS_WEIGHTS_BORGES, a, s);
-        NS_TRY(check_launch(ctx, 1));
+        NS_TRY(xstage(ctx, st, in[st], out[st], cur, nxt, true, Planes()));
         std::swap(ctx->W, ctx->W2);
-        prof_mark(ctx, NS_PROF_XFACE_UPDATE);
     }
-    ctx->parity ^= 1;
-    ctx->fused_ready = true;
-    ctx->w_next_ready = true;
-    ctx->u_valid = true;
-    ctx->w_valid = false;
-    ctx->steps++;
+    end_xstep(ctx);
     return NS_OK;
 }
 
@@ -639,6 +667,11 @@ void ns_destroy(ns_ctx* ctx) {
     cudaFree(ctx->diag);
     cudaFree(ctx->clock);
     if (ctx->sensor) sensor_destroy(ctx->sensor);
+    if (ctx->copy) {
+        cudaStreamSynchronize(ctx->copy);
+        cudaStreamDestroy(ctx->copy);
+    }
+    for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
 }
@@ -834,9 +867,184 @@ ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out) {
 
 static ns_status device_status(ns_ctx* ctx);
 
+#ifndef NS_STEP_PIPELINE
+#define NS_STEP_PIPELINE 1  // ns_time_step overlaps its host transfers with the stages
+#endif
+
+// x-planes per chunk of ns_time_step's transfer pipeline: whole marches of the
+// TMA viscous kernel and of the TMA x-march
+static int pipe_chunk() { return std::max(xmarch_planes(), viscous_march_planes()); }
+
+static bool pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// whether ns_time_step runs time_step_pipelined: an FP64 step of do_step's
+// x-march form whose kernels all take plane ranges (TMA maps of both W
+// buffers), on a single domain, at least two chunks long, from and to pinned
+// host memory (to pageable memory a copy blocks the calling thread and
+// serialises the chunks)
+static bool pipelined(const ns_ctx* ctx, const double* W, const double* U) {
+    const ns_params& p = ctx->p;
+    if (!NS_STEP_PIPELINE || !NS_XUPD_TMA || !ctx->xfused || ctx->fused || slab(ctx) || p.sensor) return false;
+    if (!ctx->tma[0].ok || !ctx->tma[1].ok || p.nx < 2 * pipe_chunk()) return false;
+    if (p.diffusion == NS_DIFF_CENTERED && (ctx->c.order > NS_VISC_TMA_MAX_ORDER || !(phys(ctx) || NS_VISC_TMA_REF)))
+        return false;
+    return pinned(W) && (!U || pinned(U));
+}
+
+static ns_status ensure_pipe(ns_ctx* ctx, int nev) {
+    if (!ctx->copy) NS_CUDA(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+    while ((int)ctx->ev.size() < nev) {
+        cudaEvent_t e;
+        NS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        ctx->ev.push_back(e);
+    }
+    return NS_OK;
+}
+
+// ns_time_step's upload, do_step and finalize_w + download of W with the host
+// transfers overlapped.  W arrives in chunks of x-planes on the copy stream,
+// and the first stage's per-plane work (layout transpose, U = cons(W) with the
+// step's CFL minimum, the face halos along y and z, W = prim(U), the y- and
+// z-face fluxes) runs on each chunk as it lands; the third stage runs chunk by
+// chunk (faces, viscous terms, x-march, W = prim(U), layout transpose) and each
+// finished chunk of W leaves on the copy stream while the next one computes.
+// The kernels and their per-cell arithmetic are those of the unpipelined
+// step, so the result is bit-identical.
+static ns_status time_step_pipelined_run(ns_ctx* ctx, const double* Wh, double* Wout) {
+    const ns_params& p = ctx->p;
+    cudaStream_t s = ctx->stream, cs = ctx->copy;
+    const int C = pipe_chunk(), nx = p.nx, K = (nx + C - 1) / C;
+    cudaEvent_t* ev = ctx->ev.data();  // [0, K) uploads, [K, 2K) downloads, [2K] start, [2K+1] end
+    const size_t plane = (size_t)(p.ny + 2 * NS_NGC) * (p.nz + 2 * NS_NGC) * NS_NQ;  // doubles per AoS x-plane
+    // chunk c: interior planes [c C, min((c + 1) C, nx)); its halo'd span adds the
+    // x ghost planes to the first and the last chunk
+    auto interior = [&](int c) {
+        Planes pl;
+        pl.lo = c * C;
+        pl.n = std::min(C, nx - c * C);
+        return pl;
+    };
+    auto halo_interior = [&](int c) {
+        Planes pl = interior(c);
+        pl.lo += NG;
+        return pl;
+    };
+    auto span = [&](int c) {
+        Planes pl;
+        pl.lo = c == 0 ? 0 : c * C + NG;
+        const int hi = c == K - 1 ? nx + 2 * NG : (c + 1) * C + NG;
+        pl.n = hi - pl.lo;
+        return pl;
+    };
+    Planes ghost_lo, ghost_hi;
+    ghost_lo.lo = 0;
+    ghost_lo.n = NG;
+    ghost_hi.lo = nx + NG;
+    ghost_hi.n = NG;
+
+    // upload: the copy stream follows the compute stream's earlier use of the staging buffer
+    NS_CUDA(cudaEventRecord(ev[2 * K], s));
+    NS_CUDA(cudaStreamWaitEvent(cs, ev[2 * K], 0));
+    for (int c = 0; c < K; c++) {
+        const Planes sp = span(c);
+        NS_CUDA(cudaMemcpyAsync(ctx->stage + sp.lo * plane, Wh + sp.lo * plane, sp.n * plane * sizeof(double),
+                                cudaMemcpyHostToDevice, cs));
+        NS_CUDA(cudaEventRecord(ev[c], cs));
+    }
+    ctx->w_valid = true;
+    ctx->u_valid = false;
+    ctx->fused_ready = ctx->halos_stale = false;
+    ctx->flags_valid = false;
+    unsigned long long* cur = ctx->slot + ctx->parity;
+    unsigned long long* nxt = ctx->slot + (ctx->parity ^ 1);
+    NS_CUDA(cudaMemsetAsync(cur, 0xFF, sizeof(unsigned long long), s));
+    NS_CUDA(cudaMemsetAsync(nxt, 0xFF, sizeof(unsigned long long), s));
+
+    // stage 1 (U0 -> U): per chunk as it lands
+    for (int c = 0; c < K; c++) {
+        const Planes sp = span(c);
+        NS_CUDA(cudaStreamWaitEvent(s, ev[c], 0));
+        launch_aos_to_soa(ctx->stage, ctx->W, ctx->box, s, sp);
+        launch_step_begin(false, phys(ctx), ctx->W, ctx->U, ctx->U0, ctx->box, ctx->c, cur, s, sp);
+        launch_fill_prim(ctx->W, ctx->U0, ctx->box, ctx->c, s, ctx->U, halo_interior(c));
+        NS_TRY(check_launch(ctx, 3));
+        NS_TRY(faces(ctx, 1, ctx->U0, true, interior(c)));
+    }
+    // the x ghost planes fold onto planes of other chunks
+    launch_fill_prim(ctx->W, ctx->U0, ctx->box, ctx->c, s, ctx->U, ghost_lo);
+    launch_fill_prim(ctx->W, ctx->U0, ctx->box, ctx->c, s, ctx->U, ghost_hi);
+    NS_TRY(check_launch(ctx, 2));
+    NS_TRY(xstage(ctx, 0, ctx->U0, ctx->U, cur, nxt, false, Planes()));
+    std::swap(ctx->W, ctx->W2);
+
+    // stage 2 (U -> U2)
+    launch_fill_halo(ctx->W, ctx->U, ctx->box, ctx->c, s, ctx->U2);
+    NS_TRY(check_launch(ctx, 1));
+    NS_TRY(xstage(ctx, 1, ctx->U, ctx->U2, cur, nxt, true, Planes()));
+    std::swap(ctx->W, ctx->W2);
+
+    // stage 3 (U2 -> U) chunk by chunk into W2, which then holds prim(U) on every
+    // cell (finalize_w); U's ghost cells are final after the fill
+    launch_fill_halo(ctx->W, ctx->U2, ctx->box, ctx->c, s, ctx->U);
+    launch_prim_all(ctx->W2, ctx->U, ctx->box, ctx->c, s, ghost_lo);
+    launch_prim_all(ctx->W2, ctx->U, ctx->box, ctx->c, s, ghost_hi);
+    NS_TRY(check_launch(ctx, 3));
+    for (int c = 0; c < K; c++) {
+        NS_TRY(xstage(ctx, 2, ctx->U2, ctx->U, cur, nxt, true, interior(c)));
+        const Planes sp = span(c);
+        launch_prim_all(ctx->W2, ctx->U, ctx->box, ctx->c, s, halo_interior(c));
+        launch_soa_to_aos(ctx->W2, ctx->stage, ctx->box, s, sp);
+        NS_TRY(check_launch(ctx, 2));
+        NS_CUDA(cudaEventRecord(ev[K + c], s));
+        NS_CUDA(cudaStreamWaitEvent(cs, ev[K + c], 0));
+        NS_CUDA(cudaMemcpyAsync(Wout + sp.lo * plane, ctx->stage + sp.lo * plane, sp.n * plane * sizeof(double),
+                                cudaMemcpyDeviceToHost, cs));
+    }
+    // the compute stream's next use of the staging buffer follows the downloads
+    NS_CUDA(cudaEventRecord(ev[2 * K + 1], cs));
+    NS_CUDA(cudaStreamWaitEvent(s, ev[2 * K + 1], 0));
+    std::swap(ctx->W, ctx->W2);
+    end_xstep(ctx);
+    ctx->w_next_ready = false;  // W holds prim(U) (finalize_w)
+    ctx->w_valid = true;
+    ctx->halos_stale = false;
+    NS_CUDA(cudaStreamSynchronize(s));
+    return NS_OK;
+}
+
+static ns_status time_step_pipelined(ns_ctx* ctx, double* W) {
+    NS_TRY(ensure_stage(ctx));
+    NS_TRY(ensure_pipe(ctx, 2 * ((ctx->p.nx + pipe_chunk() - 1) / pipe_chunk()) + 2));
+    ns_status st = time_step_pipelined_run(ctx, W, W);
+    if (st != NS_OK) {
+        // no copy of the caller's array may outlive the call
+        cudaStreamSynchronize(ctx->copy);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->w_valid = ctx->u_valid = false;
+    }
+    return st;
+}
+
 ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
     if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
     if (!W) return fail(NS_ERR_INVALID_ARG, "W is NULL");
+    if (pipelined(ctx, W, U)) {
+        NS_TRY(time_step_pipelined(ctx, W));
+        double clk[2];
+        NS_CUDA(cudaMemcpyAsync(clk, ctx->clock, sizeof clk, cudaMemcpyDeviceToHost, ctx->stream));
+        if (U) NS_TRY(download(ctx, ctx->U, U));
+        NS_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (dt_out) *dt_out = clk[0];
+        NS_TRY(device_status(ctx));
+        return check_state(ctx);
+    }
     NS_TRY(upload(ctx, W, ctx->W));
     ctx->w_valid = true;
     ctx->u_valid = false;

@@ -38,10 +38,10 @@ namespace nsb {
 template <bool FROM_U, bool PHYS>
 __global__ void __launch_bounds__(128) k_step_begin(double* __restrict__ W, double* __restrict__ U,
                                                     double* __restrict__ U0, Box b, Consts c,
-                                                    unsigned long long* __restrict__ slot) {
+                                                    unsigned long long* __restrict__ slot, int ih0) {
     int kh = blockIdx.x * 32 + threadIdx.x;
     int jh = blockIdx.y * 4 + threadIdx.y;
-    int ih = blockIdx.z;
+    int ih = blockIdx.z + ih0;
     double best = INFINITY;
     if (kh < b.nz + 2 * NG && jh < b.NY) {
         long long o = b.at(ih, jh, kh);
@@ -74,10 +74,10 @@ __global__ void __launch_bounds__(128) k_step_begin(double* __restrict__ W, doub
 
 // W = prim(U) on every cell (end of TimeScheme::step, time_scheme.cpp:69)
 __global__ void __launch_bounds__(128) k_prim_all(double* __restrict__ W, const double* __restrict__ U,
-                                                  Box b, Consts c) {
+                                                  Box b, Consts c, int ih0) {
     int kh = blockIdx.x * 32 + threadIdx.x;
     int jh = blockIdx.y * 4 + threadIdx.y;
-    int ih = blockIdx.z;
+    int ih = blockIdx.z + ih0;
     if (kh >= b.nz + 2 * NG || jh >= b.NY) return;
     long long o = b.at(ih, jh, kh);
     double u[5], w[5];
@@ -129,10 +129,10 @@ __global__ void __launch_bounds__(128) k_min_dt(const double* __restrict__ W, Bo
 // then W = prim(U) on every cell (eq_of_state.cpp:61-87).
 
 __global__ void __launch_bounds__(128) k_fill_prim(double* __restrict__ W, double* __restrict__ U,
-                                                   Box b, Consts c, double* __restrict__ Uhalo) {
+                                                   Box b, Consts c, double* __restrict__ Uhalo, int ih0) {
     int kh = blockIdx.x * 32 + threadIdx.x;
     int jh = blockIdx.y * 4 + threadIdx.y;
-    int ih = blockIdx.z;
+    int ih = blockIdx.z + ih0;
     if (kh >= b.nz + 2 * NG || jh >= b.NY) return;
     int i = ih - NG, j = jh - NG, k = kh - NG;
     bool ox = i < 0 || i >= b.nx, oy = j < 0 || j >= b.ny, oz = k < 0 || k >= b.nz;
@@ -278,10 +278,10 @@ __device__ __forceinline__ void face_at(const double* __restrict__ W, const doub
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY = false>
 __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
     k_face_flux(const double* __restrict__ W, const double* __restrict__ U, Box b, Consts c,
-                TF* __restrict__ F, FaceBox fb) {
+                TF* __restrict__ F, FaceBox fb, int aa0) {
     int kk = blockIdx.x * 32 + threadIdx.x;
     int bb = blockIdx.y * 4 + threadIdx.y;
-    int aa = blockIdx.z;
+    int aa = blockIdx.z + aa0;
     if (kk >= fb.n2 - (DIR == 2) || bb >= fb.n1 - (DIR == 1)) return;
     face_at<DIR, CHAR, BORGES, PHYS, T, TF, WONLY>(W, U, b, c, F, fb, aa, bb, kk);
 }
@@ -291,9 +291,9 @@ __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF, bool WONLY = false>
 __global__ void __launch_bounds__(128, FaceMinBlocks<CHAR, T>::value)
     k_face_flux_tail(const double* __restrict__ W, const double* __restrict__ U, Box b, Consts c,
-                     TF* __restrict__ F, FaceBox fb) {
+                     TF* __restrict__ F, FaceBox fb, int aa0) {
     static_assert(DIR > 0, "x-faces have no tail plane");
-    const int r = blockIdx.x * 128 + threadIdx.x, aa = blockIdx.y;
+    const int r = blockIdx.x * 128 + threadIdx.x, aa = blockIdx.y + aa0;
     if (r >= (DIR == 1 ? fb.n2 : fb.n1)) return;
     const int bb = DIR == 1 ? fb.n1 - 1 : r, kk = DIR == 1 ? r : fb.n2 - 1;
     face_at<DIR, CHAR, BORGES, PHYS, T, TF, WONLY>(W, U, b, c, F, fb, aa, bb, kk);
@@ -756,7 +756,7 @@ struct ViscRing {
 template <int H, bool PHYS>
 __global__ void __launch_bounds__(128, ViscRing<H>::MINB)
     k_viscous_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ W, Box b, Consts c,
-                  double* __restrict__ V, long long vs, unsigned long long* __restrict__ err) {
+                  double* __restrict__ V, long long vs, unsigned long long* __restrict__ err, int seg0) {
     using VT = ViscTile<H>;
     using VR = ViscRing<H>;
     constexpr int NSLOT = VR::NSLOT, STRIDE = VR::STRIDE, QS = VR::QS, BZ = VT::BZ;
@@ -767,7 +767,7 @@ __global__ void __launch_bounds__(128, ViscRing<H>::MINB)
         if (tid == 0) atomicOr(err, 2ull);
         return;
     }
-    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = blockIdx.z * VISC_LX;
+    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = (blockIdx.z + seg0) * VISC_LX;
     const int x1 = min(x0 + VISC_LX, b.nx);
     const int k = k0 + lane, j = j0 + ty;
     const bool live = k < b.nz && j < b.ny;
@@ -1031,10 +1031,10 @@ cudaError_t launch_div_check(long long n, unsigned long long seed, unsigned long
 // (nx+6)(ny+6)(nz+6) x 5  <->  device SoA planes)
 
 __global__ void __launch_bounds__(128) k_aos_to_soa(const double* __restrict__ A, double* __restrict__ S,
-                                                    Box b) {
+                                                    Box b, int ih0) {
     int kh = blockIdx.x * 32 + threadIdx.x;
     int jh = blockIdx.y * 4 + threadIdx.y;
-    int ih = blockIdx.z;
+    int ih = blockIdx.z + ih0;
     int NZ = b.nz + 2 * NG;
     if (kh >= NZ || jh >= b.NY) return;
     long long a = (((long long)ih * b.NY + jh) * NZ + kh) * 5;
@@ -1044,10 +1044,10 @@ __global__ void __launch_bounds__(128) k_aos_to_soa(const double* __restrict__ A
 }
 
 __global__ void __launch_bounds__(128) k_soa_to_aos(const double* __restrict__ S, double* __restrict__ A,
-                                                    Box b) {
+                                                    Box b, int ih0) {
     int kh = blockIdx.x * 32 + threadIdx.x;
     int jh = blockIdx.y * 4 + threadIdx.y;
-    int ih = blockIdx.z;
+    int ih = blockIdx.z + ih0;
     int NZ = b.nz + 2 * NG;
     if (kh >= NZ || jh >= b.NY) return;
     long long a = (((long long)ih * b.NY + jh) * NZ + kh) * 5;
@@ -1175,27 +1175,27 @@ __global__ void __launch_bounds__(128) k_check_state(const double* __restrict__ 
 // ---------------------------------------------------------------------------
 // host launchers
 
-static dim3 cell_grid(const Box& b) {  // all halo'd cells
-    return dim3((b.nz + 2 * NG + 31) / 32, (b.NY + 3) / 4, b.NX);
+static dim3 cell_grid(const Box& b, const Planes& pl = Planes()) {  // all halo'd cells (of planes pl)
+    return dim3((b.nz + 2 * NG + 31) / 32, (b.NY + 3) / 4, pl.n < 0 ? b.NX : pl.n);
 }
 static dim3 interior_grid(const Box& b) {
     return dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx);
 }
 
 void launch_step_begin(bool from_u, bool phys, double* W, double* U, double* U0, const Box& b,
-                       const Consts& c, unsigned long long* slot, cudaStream_t s) {
-    dim3 blk(32, 4);
+                       const Consts& c, unsigned long long* slot, cudaStream_t s, Planes pl) {
+    const dim3 blk(32, 4), g = cell_grid(b, pl);
     if (from_u) {
-        if (phys) k_step_begin<true, true><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
-        else k_step_begin<true, false><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
+        if (phys) k_step_begin<true, true><<<g, blk, 0, s>>>(W, U, U0, b, c, slot, pl.lo);
+        else k_step_begin<true, false><<<g, blk, 0, s>>>(W, U, U0, b, c, slot, pl.lo);
     } else {
-        if (phys) k_step_begin<false, true><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
-        else k_step_begin<false, false><<<cell_grid(b), blk, 0, s>>>(W, U, U0, b, c, slot);
+        if (phys) k_step_begin<false, true><<<g, blk, 0, s>>>(W, U, U0, b, c, slot, pl.lo);
+        else k_step_begin<false, false><<<g, blk, 0, s>>>(W, U, U0, b, c, slot, pl.lo);
     }
 }
 
-void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s) {
-    k_prim_all<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c);
+void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s, Planes pl) {
+    k_prim_all<<<cell_grid(b, pl), dim3(32, 4), 0, s>>>(W, U, b, c, pl.lo);
 }
 
 void launch_cons_all(const double* W, double* U, const Box& b, const Consts& c, cudaStream_t s) {
@@ -1214,95 +1214,100 @@ void launch_fill_halo(double* W, double* U, const Box& b, const Consts& c, cudaS
     k_fill_halo<<<dim3((unsigned)((3 * area + 127) / 128), 6), 128, 0, s>>>(W, U, b, c, Uhalo);
 }
 
-void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s, double* Uhalo) {
-    k_fill_prim<<<cell_grid(b), dim3(32, 4), 0, s>>>(W, U, b, c, Uhalo);
+void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s, double* Uhalo,
+                      Planes pl) {
+    k_fill_prim<<<cell_grid(b, pl), dim3(32, 4), 0, s>>>(W, U, b, c, Uhalo, pl.lo);
 }
 
+// x-planes of the face grid: all fb.n0, or the planes pl of the y- and z-faces
 template <int DIR, bool CHAR, bool BORGES, bool PHYS, typename T, typename TF>
 static void face_one(const double* W, const double* U, const Box& b, const Consts& c, void* F,
-                     const FaceBox& fb, cudaStream_t s, bool w_only) {
-    const dim3 grid((fb.n2 - (DIR == 2) + 31) / 32, (fb.n1 - (DIR == 1) + 3) / 4, fb.n0);
-    const dim3 tail(((DIR == 1 ? fb.n2 : fb.n1) + 127) / 128, fb.n0);
+                     const FaceBox& fb, cudaStream_t s, bool w_only, Planes pl) {
+    const int np = (DIR > 0 && pl.n >= 0) ? pl.n : fb.n0, a0 = (DIR > 0 && pl.n >= 0) ? pl.lo : 0;
+    const dim3 grid((fb.n2 - (DIR == 2) + 31) / 32, (fb.n1 - (DIR == 1) + 3) / 4, np);
+    const dim3 tail(((DIR == 1 ? fb.n2 : fb.n1) + 127) / 128, np);
     if constexpr (sizeof(T) == 8 && DIR > 0) {
         if (w_only) {
-            k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF, true><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
-            k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF, true><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb);
+            k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF, true><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb, a0);
+            k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF, true><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb, a0);
             return;
         }
     }
-    k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb);
+    k_face_flux<DIR, CHAR, BORGES, PHYS, T, TF><<<grid, dim3(32, 4), 0, s>>>(W, U, b, c, (TF*)F, fb, a0);
     if constexpr (DIR > 0)
-        k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb);
+        k_face_flux_tail<DIR, CHAR, BORGES, PHYS, T, TF><<<tail, 128, 0, s>>>(W, U, b, c, (TF*)F, fb, a0);
 }
 
 template <int DIR, bool CHAR, bool BORGES, bool PHYS>
-static void tail_one(const double* W, const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s) {
-    const dim3 tail(((DIR == 1 ? fb.n2 : fb.n1) + 127) / 128, fb.n0);
-    k_face_flux_tail<DIR, CHAR, BORGES, PHYS, double, double, true><<<tail, 128, 0, s>>>(W, W, b, c, (double*)F, fb);
+static void tail_one(const double* W, const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s,
+                     Planes pl) {
+    const dim3 tail(((DIR == 1 ? fb.n2 : fb.n1) + 127) / 128, pl.n < 0 ? fb.n0 : pl.n);
+    k_face_flux_tail<DIR, CHAR, BORGES, PHYS, double, double, true><<<tail, 128, 0, s>>>(W, W, b, c, (double*)F, fb,
+                                                                                      pl.n < 0 ? 0 : pl.lo);
 }
 
 template <int DIR>
 static void tail_dispatch(bool chr, bool borges, bool phys, const double* W, const Box& b, const Consts& c, void* F,
-                          const FaceBox& fb, cudaStream_t s) {
+                          const FaceBox& fb, cudaStream_t s, Planes pl) {
     if (chr) {
         if (borges) {
-            if (phys) tail_one<DIR, true, true, true>(W, b, c, F, fb, s);
-            else tail_one<DIR, true, true, false>(W, b, c, F, fb, s);
+            if (phys) tail_one<DIR, true, true, true>(W, b, c, F, fb, s, pl);
+            else tail_one<DIR, true, true, false>(W, b, c, F, fb, s, pl);
         } else {
-            if (phys) tail_one<DIR, true, false, true>(W, b, c, F, fb, s);
-            else tail_one<DIR, true, false, false>(W, b, c, F, fb, s);
+            if (phys) tail_one<DIR, true, false, true>(W, b, c, F, fb, s, pl);
+            else tail_one<DIR, true, false, false>(W, b, c, F, fb, s, pl);
         }
     } else {
         if (borges) {
-            if (phys) tail_one<DIR, false, true, true>(W, b, c, F, fb, s);
-            else tail_one<DIR, false, true, false>(W, b, c, F, fb, s);
+            if (phys) tail_one<DIR, false, true, true>(W, b, c, F, fb, s, pl);
+            else tail_one<DIR, false, true, false>(W, b, c, F, fb, s, pl);
         } else {
-            if (phys) tail_one<DIR, false, false, true>(W, b, c, F, fb, s);
-            else tail_one<DIR, false, false, false>(W, b, c, F, fb, s);
+            if (phys) tail_one<DIR, false, false, true>(W, b, c, F, fb, s, pl);
+            else tail_one<DIR, false, false, false>(W, b, c, F, fb, s, pl);
         }
     }
 }
 
 void launch_face_tail_w(int dir, bool chr, bool borges, bool phys, const double* W, const Box& b,
-                        const Consts& c, void* F, const FaceBox& fb, cudaStream_t s) {
-    if (dir == 1) tail_dispatch<1>(chr, borges, phys, W, b, c, F, fb, s);
-    else tail_dispatch<2>(chr, borges, phys, W, b, c, F, fb, s);
+                        const Consts& c, void* F, const FaceBox& fb, cudaStream_t s, Planes pl) {
+    if (dir == 1) tail_dispatch<1>(chr, borges, phys, W, b, c, F, fb, s, pl);
+    else tail_dispatch<2>(chr, borges, phys, W, b, c, F, fb, s, pl);
 }
 
 template <int DIR, typename T, typename TF>
 static void face_dispatch(bool chr, bool borges, bool phys, const double* W, const double* U,
                           const Box& b, const Consts& c, void* F, const FaceBox& fb, cudaStream_t s,
-                          bool w_only) {
+                          bool w_only, Planes pl) {
     if (chr) {
         if (borges) {
-            if (phys) face_one<DIR, true, true, true, T, TF>(W, U, b, c, F, fb, s, w_only);
-            else face_one<DIR, true, true, false, T, TF>(W, U, b, c, F, fb, s, w_only);
+            if (phys) face_one<DIR, true, true, true, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
+            else face_one<DIR, true, true, false, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
         } else {
-            if (phys) face_one<DIR, true, false, true, T, TF>(W, U, b, c, F, fb, s, w_only);
-            else face_one<DIR, true, false, false, T, TF>(W, U, b, c, F, fb, s, w_only);
+            if (phys) face_one<DIR, true, false, true, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
+            else face_one<DIR, true, false, false, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
         }
     } else {
         if (borges) {
-            if (phys) face_one<DIR, false, true, true, T, TF>(W, U, b, c, F, fb, s, w_only);
-            else face_one<DIR, false, true, false, T, TF>(W, U, b, c, F, fb, s, w_only);
+            if (phys) face_one<DIR, false, true, true, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
+            else face_one<DIR, false, true, false, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
         } else {
-            if (phys) face_one<DIR, false, false, true, T, TF>(W, U, b, c, F, fb, s, w_only);
-            else face_one<DIR, false, false, false, T, TF>(W, U, b, c, F, fb, s, w_only);
+            if (phys) face_one<DIR, false, false, true, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
+            else face_one<DIR, false, false, false, T, TF>(W, U, b, c, F, fb, s, w_only, pl);
         }
     }
 }
 
 void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
                       const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
-                      cudaStream_t s, bool w_only) {
+                      cudaStream_t s, bool w_only, Planes pl) {
     if (fp32) {
-        if (dir == 0) face_dispatch<0, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false);
-        else if (dir == 1) face_dispatch<1, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false);
-        else face_dispatch<2, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false);
+        if (dir == 0) face_dispatch<0, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false, Planes());
+        else if (dir == 1) face_dispatch<1, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false, Planes());
+        else face_dispatch<2, float, float>(chr, borges, phys, W, U, b, c, F, fb, s, false, Planes());
     } else {
-        if (dir == 0) face_dispatch<0, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only);
-        else if (dir == 1) face_dispatch<1, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only);
-        else face_dispatch<2, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only);
+        if (dir == 0) face_dispatch<0, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only, pl);
+        else if (dir == 1) face_dispatch<1, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only, pl);
+        else face_dispatch<2, double, double>(chr, borges, phys, W, U, b, c, F, fb, s, w_only, pl);
     }
 }
 
@@ -1360,27 +1365,31 @@ static void visc_one(const double* W, const Box& b, const Consts& c, double* V, 
 
 template <int H, bool PHYS>
 static void visc_tma_one(const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V, long long vs,
-                         unsigned long long* err, cudaStream_t s) {
+                         unsigned long long* err, cudaStream_t s, Planes pl) {
     constexpr size_t bytes = ViscRing<H>::smem;
     // the attribute is per device; a refusal surfaces as the launch's error
     cudaFuncSetAttribute(k_viscous_tma<H, PHYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    const dim3 grid((b.nz + 31) / 32, (b.ny + 3) / 4, (b.nx + VISC_LX - 1) / VISC_LX);
+    // a plane range starts on a march boundary (the launcher's contract)
+    const int seg0 = pl.n < 0 ? 0 : pl.lo / VISC_LX, np = pl.n < 0 ? b.nx : pl.n;
+    const dim3 grid((b.nz + 31) / 32, (b.ny + 3) / 4, (np + VISC_LX - 1) / VISC_LX);
     k_viscous_tma<H, PHYS><<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[3 + H - 1]),
-                                                             W, b, c, V, vs, err);
+                                                             W, b, c, V, vs, err, seg0);
 }
 
 void launch_viscous_tma(int h, bool phys, const WTmaMaps& m, const double* W, const Box& b, const Consts& c, double* V,
-                        long long vs, unsigned long long* err, cudaStream_t s) {
+                        long long vs, unsigned long long* err, cudaStream_t s, Planes pl) {
     if (phys) {
-        if (h == 1) visc_tma_one<1, true>(m, W, b, c, V, vs, err, s);
-        else if (h == 2) visc_tma_one<2, true>(m, W, b, c, V, vs, err, s);
-        else visc_tma_one<3, true>(m, W, b, c, V, vs, err, s);
+        if (h == 1) visc_tma_one<1, true>(m, W, b, c, V, vs, err, s, pl);
+        else if (h == 2) visc_tma_one<2, true>(m, W, b, c, V, vs, err, s, pl);
+        else visc_tma_one<3, true>(m, W, b, c, V, vs, err, s, pl);
     } else {
-        if (h == 1) visc_tma_one<1, false>(m, W, b, c, V, vs, err, s);
-        else if (h == 2) visc_tma_one<2, false>(m, W, b, c, V, vs, err, s);
-        else visc_tma_one<3, false>(m, W, b, c, V, vs, err, s);
+        if (h == 1) visc_tma_one<1, false>(m, W, b, c, V, vs, err, s, pl);
+        else if (h == 2) visc_tma_one<2, false>(m, W, b, c, V, vs, err, s, pl);
+        else visc_tma_one<3, false>(m, W, b, c, V, vs, err, s, pl);
     }
 }
+
+int viscous_march_planes() { return VISC_LX; }
 
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
                     long long vs, cudaStream_t s) {
@@ -1427,11 +1436,11 @@ void launch_slab_unpack(double* U, const Box& b, int side, const double* buf, cu
     k_slab_unpack<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(U, b, side, buf);
 }
 
-void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s) {
-    k_aos_to_soa<<<cell_grid(b), dim3(32, 4), 0, s>>>(A, S, b);
+void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s, Planes pl) {
+    k_aos_to_soa<<<cell_grid(b, pl), dim3(32, 4), 0, s>>>(A, S, b, pl.lo);
 }
-void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s) {
-    k_soa_to_aos<<<cell_grid(b), dim3(32, 4), 0, s>>>(S, A, b);
+void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s, Planes pl) {
+    k_soa_to_aos<<<cell_grid(b, pl), dim3(32, 4), 0, s>>>(S, A, b, pl.lo);
 }
 void launch_diagnostics(const double* U, const Box& b, const Consts& c, double* acc, cudaStream_t s) {
     k_diagnostics<<<interior_grid(b), dim3(32, 4), 0, s>>>(U, b, c, acc);

@@ -81,9 +81,22 @@ cudaError_t gate_correct(const FusedArgs& a, const GateLists& L, void* const F[3
 
 cudaError_t launch_fma_probe(bool fp64, int blocks, int iters, void* sink, cudaStream_t s);
 
+// A range of x-planes [lo, lo + n) for the launchers that take one (n < 0: all
+// planes).  The cell kernels (step begin, prim, fill, layout transposes) count
+// halo'd planes (0 .. nx+5); the y/z-face, viscous and x-march kernels count
+// interior planes (0 .. nx-1), and for the marched kernels (viscous, x-march)
+// lo is a multiple of their march length and lo + n is one too or nx.
+struct Planes {
+    int lo = 0, n = -1;
+};
+// march lengths along x of the TMA viscous kernel and of the TMA x-march
+int viscous_march_planes();
+int xmarch_planes();
+
 void launch_step_begin(bool from_u, bool phys, double* W, double* U, double* U0, const Box& b,
-                       const Consts& c, unsigned long long* slot, cudaStream_t s);
-void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s);
+                       const Consts& c, unsigned long long* slot, cudaStream_t s, Planes pl = Planes());
+void launch_prim_all(double* W, const double* U, const Box& b, const Consts& c, cudaStream_t s,
+                     Planes pl = Planes());
 void launch_cons_all(const double* W, double* U, const Box& b, const Consts& c, cudaStream_t s);
 void launch_min_dt(bool phys, const double* W, const Box& b, const Consts& c, unsigned long long* slot,
                    cudaStream_t s);
@@ -92,14 +105,14 @@ void launch_fill_halo(double* W, double* U, const Box& b, const Consts& c, cudaS
                       double* Uhalo = nullptr);
 // Uhalo (nullable) receives the same face-halo values as U
 void launch_fill_prim(double* W, double* U, const Box& b, const Consts& c, cudaStream_t s,
-                      double* Uhalo = nullptr);
+                      double* Uhalo = nullptr, Planes pl = Planes());
 // w_only (FP64 y- and z-faces of a time step, where W = prim(U)): U = cons(W)
 void launch_face_flux(int dir, bool chr, bool borges, bool phys, bool fp32, const double* W,
                       const double* U, const Box& b, const Consts& c, void* F, const FaceBox& fb,
-                      cudaStream_t s, bool w_only = false);
+                      cudaStream_t s, bool w_only = false, Planes pl = Planes());
 // the last y or z face plane (j = ny or k = nz) of an FP64 time step (W only)
 void launch_face_tail_w(int dir, bool chr, bool borges, bool phys, const double* W, const Box& b,
-                        const Consts& c, void* F, const FaceBox& fb, cudaStream_t s);
+                        const Consts& c, void* F, const FaceBox& fb, cudaStream_t s, Planes pl = Planes());
 // TMA tensor maps of one W buffer (ns_tma.cu): map[0] the y-face tiles, map[1]
 // the z-face tiles, map[2] the x-march's planes, map[3 + h - 1] the planes of the
 // marched viscous kernel of half-width h (CD-2h); each holds a CUtensorMap
@@ -127,7 +140,7 @@ bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b);
 // W that m maps, then the last face plane; *err receives 1 if a wait ran out
 void launch_face_flux_tma(int dir, bool chr, bool borges, bool phys, const WTmaMaps& m, const double* W,
                           const Box& b, const Consts& c, void* F, const FaceBox& fb, int sms,
-                          unsigned long long* err, cudaStream_t s);
+                          unsigned long long* err, cudaStream_t s, Planes pl = Planes());
 // largest ulp distance between div_pos_nr and the IEEE quotient over n draws
 cudaError_t launch_div_check(long long n, unsigned long long seed, unsigned long long* max_ulp, cudaStream_t s);
 // one block waits (bounded) on an mbarrier phase nothing completes; out[0] = 1
@@ -139,7 +152,7 @@ void launch_xface_update(bool chr, bool borges, const UpdateArgs& a, cudaStream_
 // the same with the x-stencil's W from TMA-loaded planes of the W that m maps
 // (a.W is that W); *err receives 1 if a wait ran out
 void launch_xface_update_tma(bool chr, bool borges, const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err,
-                             cudaStream_t s);
+                             cudaStream_t s, Planes pl = Planes());
 // viscous terms (components 1..4) of every interior cell into V (plane stride
 // vs >= nx ny nz), half-width h = order/2 of the centered scheme
 void launch_viscous(int h, bool phys, const double* W, const Box& b, const Consts& c, double* V,
@@ -147,12 +160,12 @@ void launch_viscous(int h, bool phys, const double* W, const Box& b, const Const
 // the same from TMA-loaded planes of the W that m maps, marched along x
 // (half-width h = 1, 2, 3); *err receives 1 if a wait ran out
 void launch_viscous_tma(int h, bool phys, const WTmaMaps& m, const double* W, const Box& b, const Consts& c,
-                        double* V, long long vs, unsigned long long* err, cudaStream_t s);
+                        double* V, long long vs, unsigned long long* err, cudaStream_t s, Planes pl = Planes());
 // slab halo exchange: pack the outer interior planes of a side / unpack into its ghost planes
 void launch_slab_pack(const double* U, const Box& b, int side, double* buf, cudaStream_t s);
 void launch_slab_unpack(double* U, const Box& b, int side, const double* buf, cudaStream_t s);
-void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s);
-void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s);
+void launch_aos_to_soa(const double* A, double* S, const Box& b, cudaStream_t s, Planes pl = Planes());
+void launch_soa_to_aos(const double* S, double* A, const Box& b, cudaStream_t s, Planes pl = Planes());
 // interior cells of A (W if prim, else U) that are non-finite or have rho <= 0 or p <= 0,
 // added to *count
 void launch_check_state(const double* A, bool prim, const Box& b, const Consts& c,

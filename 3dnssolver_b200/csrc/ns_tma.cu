@@ -82,18 +82,18 @@ struct TmaFaceMinBlocks {
 template <int DIR, bool CHAR, bool BORGES, bool PHYS>
 __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
     k_face_flux_tma(const __grid_constant__ CUtensorMap map, Box b, Consts c, double* __restrict__ F, FaceBox fb,
-                    unsigned long long* __restrict__ err) {
+                    unsigned long long* __restrict__ err, int x0, int xn) {
     using FT = FaceTile<DIR>;
     using TD = FaceTileDims<DIR>;
     __shared__ __align__(128) double buf[2 * TD::STRIDE];
     __shared__ __align__(8) unsigned long long full[2];
     const int lane = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + lane;
     const int nzt = (b.nz + 31) / 32, nyt = (b.ny + 3) / 4;
-    const int tiles = b.nx * nyt * nzt;  // the host keeps this below 2^31
+    const int tiles = xn * nyt * nzt;  // x-planes x0 .. x0+xn-1; the host keeps this below 2^31
     const int G = gridDim.x;
     const uint32_t bar[2] = {tc::smem_u32(&full[0]), tc::smem_u32(&full[1])};
     auto issue = [&](int t, int s) {
-        const int tz = t % nzt, r = t / nzt, tyi = r % nyt, aa = r / nyt;
+        const int tz = t % nzt, r = t / nzt, tyi = r % nyt, aa = x0 + r / nyt;
         const int kk0 = tz * 32, bb0 = tyi * 4;
         mbar_expect_tx(bar[s], TD::BYTES);
         tma_load_4d(tc::smem_u32(buf + s * TD::STRIDE), &map, DIR == 1 ? kk0 + 2 : kk0, DIR == 1 ? bb0 : bb0 + 3,
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
         const uint32_t par = (it >> 1) & 1;
         const bool ok = tc::mbar_wait(bar[s], par, kTilePolls);
         if (ok) {
-            const int tz = t % nzt, r = t / nzt, tyi = r % nyt, aa = r / nyt;
+            const int tz = t % nzt, r = t / nzt, tyi = r % nyt, aa = x0 + r / nyt;
             const int kk = tz * 32 + lane, bb = tyi * 4 + ty;
             if (kk < b.nz && bb < b.ny) {
                 const double* sm = buf + s * TD::STRIDE + ty * FT::BZ + FT::Z0 + lane;
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(128, CHAR ? 2 : 3)
                        const double* __restrict__ Fz, const double* __restrict__ V, long long vs, Box b, FaceBox fy,
                        FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
                        unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
-                       double* __restrict__ clock, unsigned long long* __restrict__ err) {
+                       double* __restrict__ clock, unsigned long long* __restrict__ err, int seg0) {
     constexpr bool OPS = CHAR;  // every operand staged
     using XL = XTmaLayout<H, OPS>;
     extern __shared__ __align__(128) unsigned char xsm[];
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(128, CHAR ? 2 : 3)
         if (t == 0) atomicOr(err, 2ull);
         return;
     }
-    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = blockIdx.z * XT_LX;
+    const int k0 = blockIdx.x * 32, j0 = blockIdx.y * 4, x0 = (blockIdx.z + seg0) * XT_LX;
     const int k = k0 + lane, j = j0 + ty;
     const int x1 = min(x0 + XT_LX, b.nx);
     const bool live = k < b.nz && j < b.ny;
@@ -402,77 +402,83 @@ bool w_tma_encode(WTmaMaps* m, const double* W, const Box& b) {
 
 template <int DIR, bool CHAR, bool BORGES, bool PHYS>
 static void tma_one(const WTmaMaps& m, const Box& b, const Consts& c, double* F, const FaceBox& fb, int sms,
-                    unsigned long long* err, cudaStream_t s) {
-    const int tiles = b.nx * ((b.ny + 3) / 4) * ((b.nz + 31) / 32);
+                    unsigned long long* err, cudaStream_t s, Planes pl) {
+    const int x0 = pl.n < 0 ? 0 : pl.lo, xn = pl.n < 0 ? b.nx : pl.n;
+    const int tiles = xn * ((b.ny + 3) / 4) * ((b.nz + 31) / 32);
     const int grid = std::min(tiles, sms * TmaFaceMinBlocks<CHAR>::value);
+    if (grid <= 0) return;
     const CUtensorMap& map = *reinterpret_cast<const CUtensorMap*>(m.map[DIR - 1]);
-    k_face_flux_tma<DIR, CHAR, BORGES, PHYS><<<grid, dim3(32, 4), 0, s>>>(map, b, c, F, fb, err);
+    k_face_flux_tma<DIR, CHAR, BORGES, PHYS><<<grid, dim3(32, 4), 0, s>>>(map, b, c, F, fb, err, x0, xn);
 }
 
 template <int DIR>
 static void tma_dispatch(bool chr, bool borges, bool phys, const WTmaMaps& m, const Box& b, const Consts& c,
-                         double* F, const FaceBox& fb, int sms, unsigned long long* err, cudaStream_t s) {
+                         double* F, const FaceBox& fb, int sms, unsigned long long* err, cudaStream_t s, Planes pl) {
     if (chr) {
         if (borges) {
-            if (phys) tma_one<DIR, true, true, true>(m, b, c, F, fb, sms, err, s);
-            else tma_one<DIR, true, true, false>(m, b, c, F, fb, sms, err, s);
+            if (phys) tma_one<DIR, true, true, true>(m, b, c, F, fb, sms, err, s, pl);
+            else tma_one<DIR, true, true, false>(m, b, c, F, fb, sms, err, s, pl);
         } else {
-            if (phys) tma_one<DIR, true, false, true>(m, b, c, F, fb, sms, err, s);
-            else tma_one<DIR, true, false, false>(m, b, c, F, fb, sms, err, s);
+            if (phys) tma_one<DIR, true, false, true>(m, b, c, F, fb, sms, err, s, pl);
+            else tma_one<DIR, true, false, false>(m, b, c, F, fb, sms, err, s, pl);
         }
     } else {
         if (borges) {
-            if (phys) tma_one<DIR, false, true, true>(m, b, c, F, fb, sms, err, s);
-            else tma_one<DIR, false, true, false>(m, b, c, F, fb, sms, err, s);
+            if (phys) tma_one<DIR, false, true, true>(m, b, c, F, fb, sms, err, s, pl);
+            else tma_one<DIR, false, true, false>(m, b, c, F, fb, sms, err, s, pl);
         } else {
-            if (phys) tma_one<DIR, false, false, true>(m, b, c, F, fb, sms, err, s);
-            else tma_one<DIR, false, false, false>(m, b, c, F, fb, sms, err, s);
+            if (phys) tma_one<DIR, false, false, true>(m, b, c, F, fb, sms, err, s, pl);
+            else tma_one<DIR, false, false, false>(m, b, c, F, fb, sms, err, s, pl);
         }
     }
 }
 
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
-static void xt_launch(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s) {
+static void xt_launch(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s, Planes pl) {
     constexpr size_t bytes = XTmaLayout<H, CHAR>::bytes;
     auto kern = k_xface_update_tma<CHAR, BORGES, PHYS, H, LAST>;
     // the attribute is per device; a refusal surfaces as the launch's error
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    const dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (a.b.nx + XT_LX - 1) / XT_LX);
+    // a plane range starts on a march boundary (the launcher's contract)
+    const int seg0 = pl.n < 0 ? 0 : pl.lo / XT_LX, np = pl.n < 0 ? a.b.nx : pl.n;
+    const dim3 grid((a.b.nz + 31) / 32, (a.b.ny + 3) / 4, (np + XT_LX - 1) / XT_LX);
     kern<<<grid, dim3(32, 4), bytes, s>>>(*reinterpret_cast<const CUtensorMap*>(m.map[2]), a.U,
                                           const_cast<double*>(a.U0), a.Unext, a.Wnext, (const double*)a.F[1],
                                           (const double*)a.F[2], a.V, a.vs, a.b, a.fb[1], a.fb[2], a.c, a.flags,
-                                          a.slot, LAST ? a.slot_next : nullptr, a.m1, a.m2, a.mc, a.clock, err);
+                                          a.slot, LAST ? a.slot_next : nullptr, a.m1, a.m2, a.mc, a.clock, err, seg0);
 }
 
 template <bool CHAR, bool BORGES, bool PHYS>
-static void xt_h(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s) {
+static void xt_h(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s, Planes pl) {
     const int h = a.viscous ? 1 : 0;  // the viscous terms arrive precomputed; H only sizes the operands
     if (a.slot_next) {
-        if (h) xt_launch<CHAR, BORGES, PHYS, 1, true>(a, m, err, s);
-        else xt_launch<CHAR, BORGES, PHYS, 0, true>(a, m, err, s);
+        if (h) xt_launch<CHAR, BORGES, PHYS, 1, true>(a, m, err, s, pl);
+        else xt_launch<CHAR, BORGES, PHYS, 0, true>(a, m, err, s, pl);
     } else {
-        if (h) xt_launch<CHAR, BORGES, PHYS, 1, false>(a, m, err, s);
-        else xt_launch<CHAR, BORGES, PHYS, 0, false>(a, m, err, s);
+        if (h) xt_launch<CHAR, BORGES, PHYS, 1, false>(a, m, err, s, pl);
+        else xt_launch<CHAR, BORGES, PHYS, 0, false>(a, m, err, s, pl);
     }
 }
 
 void launch_xface_update_tma(bool chr, bool borges, const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err,
-                             cudaStream_t s) {
+                             cudaStream_t s, Planes pl) {
     if (chr) {
-        if (borges) { if (a.phys) xt_h<true, true, true>(a, m, err, s); else xt_h<true, true, false>(a, m, err, s); }
-        else { if (a.phys) xt_h<true, false, true>(a, m, err, s); else xt_h<true, false, false>(a, m, err, s); }
+        if (borges) { if (a.phys) xt_h<true, true, true>(a, m, err, s, pl); else xt_h<true, true, false>(a, m, err, s, pl); }
+        else { if (a.phys) xt_h<true, false, true>(a, m, err, s, pl); else xt_h<true, false, false>(a, m, err, s, pl); }
     } else {
-        if (borges) { if (a.phys) xt_h<false, true, true>(a, m, err, s); else xt_h<false, true, false>(a, m, err, s); }
-        else { if (a.phys) xt_h<false, false, true>(a, m, err, s); else xt_h<false, false, false>(a, m, err, s); }
+        if (borges) { if (a.phys) xt_h<false, true, true>(a, m, err, s, pl); else xt_h<false, true, false>(a, m, err, s, pl); }
+        else { if (a.phys) xt_h<false, false, true>(a, m, err, s, pl); else xt_h<false, false, false>(a, m, err, s, pl); }
     }
 }
 
+int xmarch_planes() { return XT_LX; }
+
 void launch_face_flux_tma(int dir, bool chr, bool borges, bool phys, const WTmaMaps& m, const double* W,
                           const Box& b, const Consts& c, void* F, const FaceBox& fb, int sms,
-                          unsigned long long* err, cudaStream_t s) {
-    if (dir == 1) tma_dispatch<1>(chr, borges, phys, m, b, c, (double*)F, fb, sms, err, s);
-    else tma_dispatch<2>(chr, borges, phys, m, b, c, (double*)F, fb, sms, err, s);
-    launch_face_tail_w(dir, chr, borges, phys, W, b, c, F, fb, s);
+                          unsigned long long* err, cudaStream_t s, Planes pl) {
+    if (dir == 1) tma_dispatch<1>(chr, borges, phys, m, b, c, (double*)F, fb, sms, err, s, pl);
+    else tma_dispatch<2>(chr, borges, phys, m, b, c, (double*)F, fb, sms, err, s, pl);
+    launch_face_tail_w(dir, chr, borges, phys, W, b, c, F, fb, s, pl);
 }
 
 }  // namespace nsb
