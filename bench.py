@@ -708,7 +708,9 @@ def main():
     e2e_ms = rank_max(e0.elapsed_time(e1))
     e2e = {"value": job_rate(world, cells, args.e2e_steps, e2e_ms), "unit": UNIT,
            "h2d_bytes_per_step": int(Wh.nbytes), "d2h_bytes_per_step": int(Wh.nbytes),
-           "steps": args.e2e_steps, "api": "ns_time_step (TimeScheme::step drop-in), pinned host W"}
+           "steps": args.e2e_steps,
+           "api": "ns_time_step (TimeScheme::step drop-in), pinned host W; the library overlaps the chunked "
+                  "upload with the first stage and the chunked download with the third"}
     s.close()
     del Wh, Wh_t
 
