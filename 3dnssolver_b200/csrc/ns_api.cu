@@ -283,6 +283,9 @@ static void prof_mark(ns_ctx* ctx, int cls) {
 #ifndef NS_XUPD_TMA
 #define NS_XUPD_TMA 1
 #endif
+#ifndef NS_FACE_TMA_REF
+#define NS_FACE_TMA_REF 0  // the TMA face tiles for the reference semantics' y/z faces too
+#endif
 
 // the TMA tensor maps of the context's current W (FP64 steps), or null
 static const nsb::WTmaMaps* tma_maps(const ns_ctx* ctx) {
@@ -313,7 +316,8 @@ static ns_status faces(ns_ctx* ctx, int first_dir = 0, const double* Uin = nullp
             // every cell twice (local LF speed, then the split): from shared memory
             // that is 7-8% faster than the per-thread kernels on B200, which are 3-7%
             // faster for the reference semantics' single pass (256^3)
-            const nsb::WTmaMaps* m = (NS_FACE_TMA && w_only && d > 0 && phys(ctx)) ? tma_maps(ctx) : nullptr;
+            const nsb::WTmaMaps* m =
+                (NS_FACE_TMA && w_only && d > 0 && (phys(ctx) || NS_FACE_TMA_REF)) ? tma_maps(ctx) : nullptr;
             if (m)
                 launch_face_flux_tma(d, p.convection == NS_CONV_WENO5_CHAR, p.weights == NS_WEIGHTS_BORGES,
                                      phys(ctx), *m, ctx->W, ctx->box, ctx->c, ctx->F[d], ctx->fb[d], ctx->sms,

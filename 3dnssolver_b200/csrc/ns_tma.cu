@@ -168,12 +168,12 @@ __global__ void __launch_bounds__(128, TmaFaceMinBlocks<CHAR>::value)
 // for it, 8% slower for the characteristic-wise march, B200 at 256^3).
 constexpr int XT_LX = NS_XT_LX;
 
-template <int H, bool OPS = true>
+template <int H, bool OPS = true, bool OPSV = true>
 struct XTmaLayout {
     static constexpr int BZ = 34, BY = 4, QS = BZ * BY, ELEMS = 5 * QS;
     static constexpr int STRIDE = (ELEMS + 15) / 16 * 16;  // doubles per slot, 128-byte aligned
     static constexpr int NSLOT = 7;
-    static constexpr int NOP = OPS ? (H > 0 ? 34 : 30) : 10;
+    static constexpr int NOP = OPS ? (H > 0 && OPSV ? 34 : 30) : 10;
     static constexpr uint32_t TX = ELEMS * 8;
     static constexpr size_t bytes = (size_t)(NSLOT * STRIDE + (5 + NOP) * 128) * 8 + NSLOT * 8;
 };
@@ -181,16 +181,23 @@ struct XTmaLayout {
 // Two blocks per SM for the characteristic-wise march (255 registers, no
 // spills); three for the component-wise one (its 54 KB of shared memory allow
 // them, and 170 registers hold it).
+#ifndef NS_XT_MINB_CHAR
+#define NS_XT_MINB_CHAR 2
+#endif
+#ifndef NS_XT_OPS_CHAR
+#define NS_XT_OPS_CHAR 2  // characteristic-wise operands staged: 0 U0 and U, 1 and the face fluxes, 2 all
+#endif
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
-__global__ void __launch_bounds__(128, CHAR ? 2 : 3)
+__global__ void __launch_bounds__(128, CHAR ? NS_XT_MINB_CHAR : 3)
     k_xface_update_tma(const __grid_constant__ CUtensorMap map, const double* __restrict__ U, double* __restrict__ U0,
                        double* __restrict__ Uout, double* __restrict__ Wn, const double* __restrict__ Fy,
                        const double* __restrict__ Fz, const double* __restrict__ V, long long vs, Box b, FaceBox fy,
                        FaceBox fz, Consts c, int flags, const unsigned long long* __restrict__ slot,
                        unsigned long long* __restrict__ slot_next, double m1, double m2, double mc,
                        double* __restrict__ clock, unsigned long long* __restrict__ err, int seg0) {
-    constexpr bool OPS = CHAR;  // every operand staged
-    using XL = XTmaLayout<H, OPS>;
+    constexpr bool OPS = CHAR && NS_XT_OPS_CHAR >= 1;  // the face fluxes staged
+    constexpr bool OPSV = OPS && NS_XT_OPS_CHAR >= 2;  // the viscous terms too
+    using XL = XTmaLayout<H, OPS, OPSV>;
     extern __shared__ __align__(128) unsigned char xsm[];
     double* ring = reinterpret_cast<double*>(xsm);  // [NSLOT][5][BY][BZ]
     double* fprev = ring + XL::NSLOT * XL::STRIDE;   // [5][128]
@@ -262,7 +269,7 @@ __global__ void __launch_bounds__(128, CHAR ? 2 : 3)
                     }
                 }
             }
-            if constexpr (H > 0 && OPS) {
+            if constexpr (H > 0 && OPSV) {
                 const long long e = ((long long)i * b.ny + j) * b.nz + k;
 #pragma unroll
                 for (int q = 0; q < 4; q++) cp_async8(&opnd[(30 + q) * 128 + t], V + q * vs + e);
@@ -312,7 +319,7 @@ __global__ void __launch_bounds__(128, CHAR ? 2 : 3)
         if constexpr (H > 0) {
 #pragma unroll
             for (int q = 1; q < 5; q++)
-                r[q] += OPS ? opnd[(29 + q) * 128 + t] : V[(q - 1) * vs + ((long long)i * b.ny + j) * b.nz + k];
+                r[q] += OPSV ? opnd[(29 + q) * 128 + t] : V[(q - 1) * vs + ((long long)i * b.ny + j) * b.nz + k];
         }
         double un[5], w[5];
 #pragma unroll
@@ -435,7 +442,7 @@ static void tma_dispatch(bool chr, bool borges, bool phys, const WTmaMaps& m, co
 
 template <bool CHAR, bool BORGES, bool PHYS, int H, bool LAST>
 static void xt_launch(const UpdateArgs& a, const WTmaMaps& m, unsigned long long* err, cudaStream_t s, Planes pl) {
-    constexpr size_t bytes = XTmaLayout<H, CHAR>::bytes;
+    constexpr size_t bytes = XTmaLayout<H, CHAR && NS_XT_OPS_CHAR >= 1, NS_XT_OPS_CHAR >= 2>::bytes;
     auto kern = k_xface_update_tma<CHAR, BORGES, PHYS, H, LAST>;
     // the attribute is per device; a refusal surfaces as the launch's error
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
