@@ -82,6 +82,8 @@ def load_library():
         "ns_wait_selftest": ([ctypes.c_uint, ctypes.POINTER(ctypes.c_int), dp], st),
         "ns_div_selftest": ([ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong)], st),
         "ns_get_dt": ([C, dp, dp], st),
+        "ns_host_register": ([ctypes.c_void_p, ctypes.c_size_t], st),
+        "ns_host_unregister": ([ctypes.c_void_p], st),
     }
     for name, (args, res) in protos.items():
         f = getattr(L, name)
@@ -139,6 +141,17 @@ def wait_selftest(polls=4096):
     r, t = ctypes.c_int(), ctypes.c_double()
     _check(load_library().ns_wait_selftest(int(polls), ctypes.byref(r), ctypes.byref(t)), "ns_wait_selftest")
     return bool(r.value), t.value
+
+
+def host_register(a):
+    """Page-locks the storage of numpy array a (ns_host_register), so that
+    Solver.time_step on it overlaps its copies with the stages; release it with
+    host_unregister before the array goes."""
+    _check(load_library().ns_host_register(ctypes.c_void_p(a.ctypes.data), a.nbytes), "ns_host_register")
+
+
+def host_unregister(a):
+    _check(load_library().ns_host_unregister(ctypes.c_void_p(a.ctypes.data)), "ns_host_unregister")
 
 
 def div_selftest(n=1 << 22, seed=7):

@@ -14,6 +14,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "ns_b200.h"
 
@@ -66,14 +67,17 @@ public:
     explicit Context(const Params& p) {
         ns_params q = to_ns_params(p);
         check(ns_create(&q, &m_ctx), "ns_create");
+        m_elems = ns_host_array_elems(&q);
     }
     ~Context() { ns_destroy(m_ctx); }
     Context(const Context&) = delete;
     Context& operator=(const Context&) = delete;
     ns_ctx* get() const { return m_ctx; }
+    size_t host_elems() const { return m_elems; }  // doubles of one host Array4d
 
 private:
     ns_ctx* m_ctx = nullptr;
+    size_t m_elems = 0;
 };
 
 // ConvectionScheme::solve(grid, W, U, R): R += convective residual on the GPU
@@ -103,18 +107,34 @@ private:
 
 // TimeScheme::step (src/time_scheme.hpp:25-29) with the whole step on the GPU:
 // W is uploaded, stepped and downloaded with U each call.
+// With pin (the default) the first step page-locks the Domain's W and U
+// (ns_host_register), so that every step overlaps its copies with the stages;
+// the destructor releases them, so destroy the scheme before the Domain.  A
+// range that cannot be locked is used as it is.
 class GpuTimeScheme {
 public:
-    explicit GpuTimeScheme(Context& c) : m_c(c) {}
+    explicit GpuTimeScheme(Context& c, bool pin = true) : m_c(c), m_pin(pin) {}
+    ~GpuTimeScheme() {
+        for (double* p : m_pinned) ns_host_unregister(p);
+    }
+    GpuTimeScheme(const GpuTimeScheme&) = delete;
+    GpuTimeScheme& operator=(const GpuTimeScheme&) = delete;
     void step(Domain& d, const Grid&, const Communicator&, ConvectionScheme*, DiffusionScheme*) {
-        check(ns_time_step(m_c.get(), data(d.get_NS_primitive_array()),
-                           data(d.get_NS_conservative_array()), &m_dt),
-              "ns_time_step");
+        double* W = data(d.get_NS_primitive_array());
+        double* U = data(d.get_NS_conservative_array());
+        if (m_pin) {
+            m_pin = false;
+            for (double* p : {W, U})
+                if (ns_host_register(p, m_c.host_elems() * sizeof(double)) == NS_OK) m_pinned.push_back(p);
+        }
+        check(ns_time_step(m_c.get(), W, U, &m_dt), "ns_time_step");
     }
     double get_dt() const { return m_dt; }
 
 private:
     Context& m_c;
+    bool m_pin;
+    std::vector<double*> m_pinned;
     double m_dt = 0.0;
 };
 

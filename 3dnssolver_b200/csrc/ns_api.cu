@@ -1065,6 +1065,18 @@ ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out) {
     return check_state(ctx);
 }
 
+ns_status ns_host_register(void* ptr, size_t bytes) {
+    if (!ptr || bytes == 0) return fail(NS_ERR_INVALID_ARG, "ptr is NULL or bytes is 0");
+    NS_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    return NS_OK;
+}
+
+ns_status ns_host_unregister(void* ptr) {
+    if (!ptr) return fail(NS_ERR_INVALID_ARG, "ptr is NULL");
+    NS_CUDA(cudaHostUnregister(ptr));
+    return NS_OK;
+}
+
 ns_status ns_advance(ns_ctx* ctx, int nsteps) {
     if (!ctx) return fail(NS_ERR_INVALID_ARG, "ctx is NULL");
     if (nsteps < 0) return fail(NS_ERR_INVALID_ARG, "nsteps must be >= 0");

@@ -160,8 +160,17 @@ NS_API ns_status ns_rhs(ns_ctx* ctx, const double* W, double* R, int terms);
 NS_API ns_status ns_compute_dt(ns_ctx* ctx, const double* W, double* dt_out);
 /* TimeScheme::step (src/time_scheme.hpp:25-29, src/time_scheme.cpp:3-70): one SSP-RK3
  * step of host W (in/out) and U (out, may be NULL); dt_out receives the step's dt.
- * Host <-> device copies are part of the call. */
+ * Host <-> device copies are part of the call.  When W (and U) lie in page-locked
+ * host memory (cudaHostAlloc, or ns_host_register), an FP64 step on a single
+ * domain overlaps the copies with the stages: W goes up in chunks of x-planes under
+ * the first stage and comes down in chunks during the third.  The result is the
+ * same bit for bit. */
 NS_API ns_status ns_time_step(ns_ctx* ctx, double* W, double* U, double* dt_out);
+/* Page-locks (cudaHostRegister) / releases a host range, for hosts that do not
+ * link the CUDA runtime themselves, so that ns_time_step on arrays inside it
+ * overlaps its copies.  No context needed; release before freeing the memory. */
+NS_API ns_status ns_host_register(void* ptr, size_t bytes);
+NS_API ns_status ns_host_unregister(void* ptr);
 
 /* ---- device-resident time loop -------------------------------------------- */
 /* Runs nsteps steps of TimeScheme::step on the device-resident state (the Driver

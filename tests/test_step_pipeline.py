@@ -101,3 +101,23 @@ def test_pipelined_time_step_without_u_download():
         assert _same(Wa, Wb) and np.isfinite(interior(Wb)).all()
         assert _same(a.download_conservative(), b.download_conservative())
         del Wb, tW
+
+
+def test_registered_host_arrays_take_the_pipeline():
+    """ns_host_register page-locks a caller's pageable array: the step on it
+    takes the pipelined path (its chunked launches) and gives the same bits."""
+    p = pkg.make_params(130, 10, 12, convection=pkg.CONV_WENO5_CHAR, diffusion_order=2, mu=0.02, cfl=0.2,
+                        semantics=pkg.SEM_PHYSICAL)
+    W0 = wl.random_field(p, seed=37, smooth=False)
+    with pkg.Solver(p) as a, pkg.Solver(p) as b:
+        Wa = W0.copy()
+        Wb = W0.copy()
+        pkg.host_register(Wb)
+        try:
+            for _ in range(2):
+                a.time_step(Wa)
+                b.time_step(Wb)
+            assert _same(Wa, Wb) and np.isfinite(interior(Wb)).all()
+            assert b.launches > a.launches
+        finally:
+            pkg.host_unregister(Wb)
