@@ -113,3 +113,12 @@ def test_host_buffers_of_the_wrong_shape_or_type_are_refused_on_the_host():
     ro.flags.writeable = False
     with pytest.raises(ValueError):
         pkg.check_host_array(ro, shape, writable=True)
+
+
+def test_host_register_checks_its_arguments_on_the_host():
+    L = pkg.load_library()
+    assert L.ns_host_register(None, 64) == pkg.abi.NS_ERR_INVALID_ARG
+    buf = np.zeros(8)
+    assert L.ns_host_register(ctypes.c_void_p(buf.ctypes.data), 0) == pkg.abi.NS_ERR_INVALID_ARG
+    assert L.ns_host_unregister(None) == pkg.abi.NS_ERR_INVALID_ARG
+    assert "NULL" in L.ns_last_error_string().decode()
